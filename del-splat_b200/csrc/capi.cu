@@ -1,0 +1,628 @@
+// capi.cu -- the extern "C" entry points declared in include/dsplat.h.
+//
+// Host orchestration only: argument checks, workspace carving and the launch
+// sequence of each entry point.  No device memory is allocated here; every
+// buffer comes from the caller.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+
+namespace dsplat {
+// kernels and launchers defined in the other translation units
+__global__ void k_gauss_project_ref(uint32_t, const float*, const float*, const float*, const float*, int, int, float*,
+                                    float*, float*);
+__global__ void k_circle_project_ref(uint32_t, const float*, const float*, int, int, float, float*, float*);
+__global__ void k_prep_tiles(uint32_t, const float*, const float*, const float*, int, int, int, uint2*, uint32_t*,
+                             uint32_t*);
+__global__ void k_fused_project(uint32_t, uint32_t, int, const float*, const float*, const float*, const float*,
+                                const float*, const ViewBatch, float4*, uint2*, uint32_t*, uint32_t*);
+__global__ void k_project_bwd(uint32_t, int, const float*, const float*, const float*, const float*, const ViewBatch,
+                              const float4*, float*, float*, float*, float*, float*);
+__global__ void k_adam(size_t, float*, const float*, float*, float*, float, float, float, float, float, float);
+__global__ void k_iota_pad(uint32_t*, uint32_t*, uint32_t, uint32_t, uint32_t);
+__global__ void k_gather_counts(const uint32_t*, const uint32_t*, uint32_t, uint32_t, uint32_t, uint32_t*);
+__global__ void k_emit_pairs(const uint32_t*, const uint32_t*, const uint32_t*, const uint2*, uint32_t, uint32_t,
+                             uint32_t, const ViewBatch, uint64_t, uint32_t*, uint32_t*, uint32_t*);
+__global__ void k_item_ranges(const uint32_t*, const uint32_t*, uint64_t, uint32_t, uint32_t*);
+__global__ void k_copy_total(const uint32_t*, size_t, uint32_t*);
+__global__ void k_make_keys64(const uint32_t*, const uint32_t*, const float*, const uint32_t*, uint64_t, uint64_t*);
+__global__ void k_fill_u64(uint64_t*, size_t, uint64_t);
+__global__ void k_point_zbuf(uint32_t, const float*, int, int, uint64_t*);
+__global__ void k_point_resolve(size_t, const uint64_t*, const float*, const float*, float*, float*, int32_t*);
+__global__ void k_circle_zbuf(uint32_t, const float*, const float*, int, int, int, uint64_t*);
+__global__ void k_circle_resolve(size_t, const uint64_t*, const void*, int, void*, int32_t*);
+
+size_t scan_tmp_words(size_t n);
+size_t radix_hist_words(size_t n);
+cudaError_t exclusive_scan(cudaStream_t, const uint32_t*, uint32_t*, size_t, uint32_t*);
+cudaError_t radix_sort(cudaStream_t, uint32_t*, uint32_t*, uint32_t*, uint32_t*, size_t, const uint32_t*, int, uint32_t,
+                       uint32_t*, uint32_t*, bool*);
+cudaError_t raster_fwd(cudaStream_t, const ViewBatch&, uint32_t, const float4*, const uint32_t*, const uint32_t*,
+                       uint32_t*, float*, float*, uint32_t*, const float*, float*, float*);
+cudaError_t raster_bwd(cudaStream_t, const ViewBatch&, uint32_t, const float4*, const uint32_t*, const uint32_t*,
+                       uint32_t*, const float*, const float*, const uint32_t*, float4*);
+cudaError_t raster_fwd_aos(cudaStream_t, int, int, int, float*, const float*, const float*, const float*, const float*,
+                           const float*, const uint32_t*, const uint32_t*, float*, uint32_t*);
+cudaError_t circle_splat_tiles(cudaStream_t, int, int, int, float*, const float*, const float*, const float*,
+                               const uint32_t*, const uint32_t*);
+
+__global__ void k_one_minus(const float* __restrict__ T, float* __restrict__ out, size_t n) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = 1.f - T[i];
+}
+
+__global__ void k_copy_u32_count(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                                 const uint32_t* __restrict__ count_ptr, uint64_t capacity) {
+  uint32_t cnt = *count_ptr;
+  if (cnt > capacity) cnt = uint32_t(capacity);
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < cnt; i += size_t(gridDim.x) * blockDim.x)
+    dst[i] = src[i];
+}
+
+namespace {
+
+thread_local std::string g_last_error;
+
+// Optional CUDA events recorded at stage boundaries of the batched calls
+// (profiling hook, dsplat_set_stage_events).
+thread_local cudaEvent_t g_stage_ev[16];
+thread_local int g_stage_n = 0;
+inline void stage_mark(cudaStream_t st, int k) {
+  if (k < g_stage_n && g_stage_ev[k]) cudaEventRecord(g_stage_ev[k], st);
+}
+
+int fail(int code, const char* msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  char buf[256];
+  snprintf(buf, sizeof(buf), "%s: %s", where, cudaGetErrorString(e));
+  g_last_error = buf;
+  return DSPLAT_ERR_CUDA;
+}
+
+#define TRY_CUDA(expr, where)                    \
+  do {                                           \
+    cudaError_t _e = (expr);                     \
+    if (_e != cudaSuccess) return cuda_fail(_e, where); \
+  } while (0)
+
+inline unsigned blocks_for(size_t n, unsigned t) { return unsigned((n + t - 1) / t); }
+inline bool ts_ok(uint32_t ts) { return ts == 8 || ts == 16 || ts == 32; }
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+inline uint32_t ceil_div(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
+inline int bits_for(uint32_t n_items) {
+  int b = 0;
+  while ((1ull << b) < uint64_t(n_items)) ++b;
+  return b;
+}
+constexpr uint32_t kSortTile = 4096;
+
+// Simple bump allocator over the caller's workspace.
+struct Carver {
+  char* base;
+  size_t off = 0;
+  explicit Carver(void* p) : base(static_cast<char*>(p)) {}
+  template <class T>
+  T* take(size_t count, size_t* off_out = nullptr) {
+    off = align_up(off, 256);
+    if (off_out) *off_out = off;
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += count * sizeof(T);
+    return p;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Single-view tile list builder shared by the Gaussian and circle entries.
+// ---------------------------------------------------------------------------
+struct TileWs {
+  uint32_t* flags;  // [0] flags, [1] total pairs
+  uint2* rect;
+  uint32_t *cnt, *dka, *dva, *dkb, *dvb, *cs, *off, *hist, *scan_tmp, *pka, *pva, *pkb;
+  size_t bytes;
+};
+
+TileWs carve_tiles(void* ws, uint32_t n, uint32_t tile_w, uint32_t tile_h, uint64_t pairs) {
+  (void)tile_w;
+  (void)tile_h;
+  const uint32_t npad = ceil_div(n > 0 ? n : 1, kSortTile) * kSortTile;
+  const size_t cap = pairs > 0 ? pairs : 1;
+  Carver c(ws);
+  TileWs t;
+  t.flags = c.take<uint32_t>(16);
+  t.rect = c.take<uint2>(n + 1);
+  t.cnt = c.take<uint32_t>(size_t(n) + 1);
+  t.dka = c.take<uint32_t>(npad);
+  t.dva = c.take<uint32_t>(npad);
+  t.dkb = c.take<uint32_t>(npad);
+  t.dvb = c.take<uint32_t>(npad);
+  t.cs = c.take<uint32_t>(size_t(npad) + 1);
+  t.off = c.take<uint32_t>(size_t(npad) + 1);
+  const size_t hw = radix_hist_words(npad > cap ? npad : cap);
+  t.hist = c.take<uint32_t>(hw);
+  const size_t sw = scan_tmp_words(hw > size_t(npad) + 1 ? hw : size_t(npad) + 1);
+  t.scan_tmp = c.take<uint32_t>(sw);
+  t.pka = c.take<uint32_t>(cap);
+  t.pva = c.take<uint32_t>(cap);
+  t.pkb = c.take<uint32_t>(cap);
+  t.bytes = c.off;
+  return t;
+}
+
+ViewBatch single_view_batch(int w, int h, int ts, uint32_t tile_w, uint32_t tile_h) {
+  ViewBatch b;
+  memset(&b, 0, sizeof(b));
+  b.num_views = 1;
+  b.ts = ts;
+  b.num_items = tile_w * tile_h;
+  b.num_pix = uint32_t(w) * uint32_t(h);
+  b.v[0].w = w;
+  b.v[0].h = h;
+  b.v[0].tile_w = int(tile_w);
+  b.v[0].tile_h = int(tile_h);
+  return b;
+}
+
+// counts only: prep + sum
+int tiles_count(cudaStream_t st, uint32_t n, const float* xyd, const float* aabb, const float* rad, uint32_t tile_w,
+                uint32_t tile_h, uint32_t ts, void* ws, size_t ws_bytes, uint64_t* num_pairs) {
+  if (!num_pairs) return fail(DSPLAT_ERR_INVALID_ARG, "num_pairs is null");
+  if (!ts_ok(ts)) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
+  TileWs t = carve_tiles(nullptr, n, tile_w, tile_h, 0);
+  if (!ws || ws_bytes < t.bytes) return fail(DSPLAT_ERR_WORKSPACE, "workspace too small");
+  t = carve_tiles(ws, n, tile_w, tile_h, 0);
+  *num_pairs = 0;
+  if (n == 0 || tile_w == 0 || tile_h == 0) return DSPLAT_OK;
+  k_prep_tiles<<<blocks_for(n, 256), 256, 0, st>>>(n, xyd, aabb, rad, int(ts), int(tile_w), int(tile_h), t.rect,
+                                                  t.dka, t.cnt); count_launch();
+  TRY_CUDA(cudaMemsetAsync(t.cnt + n, 0, sizeof(uint32_t), st), "memset");
+  TRY_CUDA(exclusive_scan(st, t.cnt, t.off, size_t(n) + 1, t.scan_tmp), "scan");
+  uint32_t total = 0;
+  TRY_CUDA(cudaMemcpyAsync(&total, t.off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "memcpy");
+  TRY_CUDA(cudaStreamSynchronize(st), "sync");
+  *num_pairs = total;
+  return DSPLAT_OK;
+}
+
+int tiles_fill(cudaStream_t st, uint32_t n, const float* xyd, const float* aabb, const float* rad, int img_w,
+               int img_h, uint32_t tile_w, uint32_t tile_h, uint32_t ts, uint32_t* tile2idx, uint32_t* idx2pnt,
+               uint64_t capacity, uint64_t* keys64, void* ws, size_t ws_bytes) {
+  if (!ts_ok(ts)) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
+  if (!tile2idx || (!idx2pnt && capacity > 0)) return fail(DSPLAT_ERR_INVALID_ARG, "null output");
+  if (n > 0 && !xyd) return fail(DSPLAT_ERR_INVALID_ARG, "null input");
+  TileWs t = carve_tiles(nullptr, n, tile_w, tile_h, capacity);
+  if (!ws || ws_bytes < t.bytes) return fail(DSPLAT_ERR_WORKSPACE, "workspace too small");
+  t = carve_tiles(ws, n, tile_w, tile_h, capacity);
+  const uint32_t T = tile_w * tile_h;
+  TRY_CUDA(cudaMemsetAsync(t.flags, 0, 16 * sizeof(uint32_t), st), "memset");
+  if (n == 0 || T == 0) {
+    TRY_CUDA(cudaMemsetAsync(tile2idx, 0, (size_t(T) + 1) * sizeof(uint32_t), st), "memset");
+    return DSPLAT_OK;
+  }
+  const uint32_t npad = ceil_div(n, kSortTile) * kSortTile;
+  ViewBatch b = single_view_batch(img_w, img_h, int(ts), tile_w, tile_h);
+  k_iota_pad<<<blocks_for(npad, 256), 256, 0, st>>>(t.dva, t.dka, n, npad, 1); count_launch();
+  k_prep_tiles<<<blocks_for(n, 256), 256, 0, st>>>(n, xyd, aabb, rad, int(ts), int(tile_w), int(tile_h), t.rect,
+                                                  t.dka, t.cnt); count_launch();
+  bool in_b = false;
+  TRY_CUDA(radix_sort(st, t.dka, t.dva, t.dkb, t.dvb, npad, nullptr, 32, 1, t.hist, t.scan_tmp, &in_b), "depth sort");
+  const uint32_t* order = in_b ? t.dvb : t.dva;
+  k_gather_counts<<<blocks_for(size_t(npad) + 1, 256), 256, 0, st>>>(order, t.cnt, n, npad, 1, t.cs); count_launch();
+  TRY_CUDA(exclusive_scan(st, t.cs, t.off, size_t(npad) + 1, t.scan_tmp), "scan");
+  k_copy_total<<<1, 32, 0, st>>>(t.off, npad, t.flags + 1); count_launch();
+  if (capacity > 0) {
+    // the caller's idx2pnt is the second value buffer of the tile sort
+    k_emit_pairs<<<blocks_for(npad, 256), 256, 0, st>>>(order, t.cs, t.off, t.rect, n, npad, 1, b, capacity, t.pka,
+                                                        t.pva, t.flags); count_launch();
+    const int bits = bits_for(T);
+    TRY_CUDA(radix_sort(st, t.pka, t.pva, t.pkb, idx2pnt, capacity, t.flags + 1, bits, 1, t.hist, t.scan_tmp, &in_b),
+             "tile sort");
+    const uint32_t* skeys = in_b ? t.pkb : t.pka;
+    if (!in_b) k_copy_u32_count<<<1024, 256, 0, st>>>(t.pva, idx2pnt, t.flags + 1, capacity); count_launch();
+    k_item_ranges<<<1184, 256, 0, st>>>(skeys, t.flags + 1, capacity, T, tile2idx); count_launch();
+    if (keys64)
+      k_make_keys64<<<1184, 256, 0, st>>>(skeys, idx2pnt, xyd, t.flags + 1, capacity, keys64); count_launch();
+  } else {
+    uint32_t* fake = t.pka;
+    TRY_CUDA(cudaMemsetAsync(fake, 0, sizeof(uint32_t), st), "memset");
+    k_item_ranges<<<1, 32, 0, st>>>(fake, fake, 0, T, tile2idx); count_launch();
+  }
+  TRY_CUDA(cudaGetLastError(), "launch");
+  return DSPLAT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched Gaussian state
+// ---------------------------------------------------------------------------
+struct BatchWs {
+  dsplat_batch_layout L;
+  uint32_t* flags;
+  float4* rec;
+  uint2* rect;
+  uint32_t *cnt, *dka, *dva, *dkb, *dvb, *cs, *off, *hist, *scan_tmp, *pka, *pva, *pkb, *pvb, *item_start;
+  float* pix_T;
+  uint32_t* pix_stop;
+  float* grad_pix;
+  float* item_loss;
+  float4* grad2d;
+  bool order_in_b, pairs_in_b;
+};
+
+int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, ViewBatch* b) {
+  if (nv < 1 || nv > DSPLAT_MAX_VIEWS) return fail(DSPLAT_ERR_INVALID_ARG, "num_views must be in [1, 32]");
+  if (!views) return fail(DSPLAT_ERR_INVALID_ARG, "views is null");
+  if (!ts_ok(uint32_t(ts))) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
+  if (n64 < 0 || n64 > int64_t(0x7fffffff)) return fail(DSPLAT_ERR_INVALID_ARG, "num_pnt out of range");
+  memset(b, 0, sizeof(*b));
+  b->num_views = nv;
+  b->ts = ts;
+  uint64_t items = 0, pix = 0;
+  for (int v = 0; v < nv; ++v) {
+    const dsplat_view& s = views[v];
+    if (s.width <= 0 || s.height <= 0 || s.width > 65535 * 8 || s.height > 65535 * 8)
+      return fail(DSPLAT_ERR_INVALID_ARG, "bad view size");
+    ViewDev& d = b->v[v];
+    memcpy(d.mvp, s.mvp, sizeof(d.mvp));
+    memcpy(d.campos, s.campos, sizeof(d.campos));
+    d.w = s.width;
+    d.h = s.height;
+    d.tile_w = (s.width + ts - 1) / ts;
+    d.tile_h = (s.height + ts - 1) / ts;
+    d.item_base = uint32_t(items);
+    d.pix_base = uint32_t(pix);
+    items += uint64_t(d.tile_w) * d.tile_h;
+    pix += uint64_t(s.width) * s.height;
+  }
+  if (items >= 0xffffffffull || pix * 3 >= 0xffffffffull) return fail(DSPLAT_ERR_INVALID_ARG, "batch too large");
+  b->num_items = uint32_t(items);
+  b->num_pix = uint32_t(pix);
+  return DSPLAT_OK;
+}
+
+BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity) {
+  const uint32_t V = uint32_t(b.num_views);
+  const uint32_t npad = ceil_div(n > 0 ? n : 1, kSortTile) * kSortTile;
+  const size_t cap = capacity > 0 ? capacity : 1;
+  const size_t VN = size_t(V) * n, Vp = size_t(V) * npad;
+  Carver c(ws);
+  BatchWs w;
+  dsplat_batch_layout& L = w.L;
+  memset(&L, 0, sizeof(L));
+  L.num_items = b.num_items;
+  L.num_pix = b.num_pix;
+  L.npad = npad;
+  L.tile_sort_bits = uint32_t(bits_for(b.num_items));
+  w.flags = c.take<uint32_t>(16, &L.off_flags);
+  w.rec = c.take<float4>(3 * VN + 3, &L.off_rec);
+  w.rect = c.take<uint2>(VN + 1, &L.off_rect);
+  w.cnt = c.take<uint32_t>(VN + 1, &L.off_cnt);
+  size_t off_a, off_b;
+  w.dka = c.take<uint32_t>(Vp);
+  w.dva = c.take<uint32_t>(Vp, &off_a);
+  w.dkb = c.take<uint32_t>(Vp);
+  w.dvb = c.take<uint32_t>(Vp, &off_b);
+  w.order_in_b = false;  // 4 passes of 8 bits end in the first buffer pair
+  L.off_order = off_a;
+  w.cs = c.take<uint32_t>(Vp + 1);
+  w.off = c.take<uint32_t>(Vp + 1);
+  const size_t hw = radix_hist_words(Vp > cap ? Vp : cap);
+  w.hist = c.take<uint32_t>(hw);
+  w.scan_tmp = c.take<uint32_t>(scan_tmp_words(hw > Vp + 1 ? hw : Vp + 1));
+  size_t ok_a, ov_a, ok_b, ov_b;
+  w.pka = c.take<uint32_t>(cap, &ok_a);
+  w.pva = c.take<uint32_t>(cap, &ov_a);
+  w.pkb = c.take<uint32_t>(cap, &ok_b);
+  w.pvb = c.take<uint32_t>(cap, &ov_b);
+  const int passes = (int(L.tile_sort_bits) + 7) / 8;
+  w.pairs_in_b = (passes % 2) == 1;
+  L.off_idx2pnt = w.pairs_in_b ? ov_b : ov_a;
+  L.off_item_key = w.pairs_in_b ? ok_b : ok_a;
+  w.item_start = c.take<uint32_t>(size_t(b.num_items) + 1, &L.off_item_start);
+  w.pix_T = c.take<float>(b.num_pix, &L.off_pix_T);
+  w.pix_stop = c.take<uint32_t>(b.num_pix, &L.off_pix_stop);
+  w.grad_pix = c.take<float>(size_t(b.num_pix) * 3, &L.off_grad_pix);
+  w.item_loss = c.take<float>(b.num_items, &L.off_item_loss);
+  w.grad2d = c.take<float4>(3 * VN + 3, &L.off_grad2d);
+  L.total_bytes = align_up(c.off, 256);
+  return w;
+}
+
+int check_params(const dsplat_gauss_params* p) {
+  if (!p) return fail(DSPLAT_ERR_INVALID_ARG, "params is null");
+  if (p->sh_degree < -1 || p->sh_degree > 3) return fail(DSPLAT_ERR_INVALID_ARG, "sh_degree must be -1..3");
+  if (p->num_pnt > 0 && (!p->means || !p->log_scales || !p->quats || !p->opacity || !p->colors))
+    return fail(DSPLAT_ERR_INVALID_ARG, "null parameter pointer");
+  return DSPLAT_OK;
+}
+
+}  // namespace
+}  // namespace dsplat
+
+using namespace dsplat;
+
+extern "C" {
+
+const char* dsplat_version(void) { return "dsplat-b200 0.1.0 (sm_100a)"; }
+const char* dsplat_last_error(void) { return g_last_error.c_str(); }
+
+int dsplat_gauss_pnt2splat3_to_pnt2splat2(dsplat_stream stream, uint32_t num_pnt, const float* pnt2xyz,
+                                          const float* pnt2scale, const float* pnt2quat, float* pnt2pixxydepth,
+                                          float* pnt2pixconvinv, float* pnt2pixaabb,
+                                          const float* transform_world2ndc, uint32_t img_w, uint32_t img_h) {
+  if (num_pnt == 0) return DSPLAT_OK;
+  if (!pnt2xyz || !pnt2scale || !pnt2quat || !pnt2pixxydepth || !pnt2pixconvinv || !pnt2pixaabb ||
+      !transform_world2ndc)
+    return fail(DSPLAT_ERR_INVALID_ARG, "null pointer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_gauss_project_ref<<<blocks_for(num_pnt, 256), 256, 0, st>>>(num_pnt, pnt2xyz, pnt2quat, pnt2scale,
+                                                                transform_world2ndc, int(img_w), int(img_h),
+                                                                pnt2pixxydepth, pnt2pixconvinv, pnt2pixaabb); count_launch();
+  TRY_CUDA(cudaGetLastError(), "k_gauss_project_ref");
+  return DSPLAT_OK;
+}
+
+size_t dsplat_tile2idx_workspace_size(uint32_t num_pnt, uint32_t tile_w, uint32_t tile_h, uint64_t num_pairs) {
+  return carve_tiles(nullptr, num_pnt, tile_w, tile_h, num_pairs).bytes;
+}
+
+int dsplat_gauss_tile2idx_count(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixaabb, uint32_t img_w,
+                                uint32_t img_h, uint32_t tile_size, void* workspace, size_t workspace_bytes,
+                                uint64_t* num_pairs) {
+  if (!ts_ok(tile_size)) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
+  if (num_pnt > 0 && !pnt2pixaabb) return fail(DSPLAT_ERR_INVALID_ARG, "null pnt2pixaabb");
+  const uint32_t tw = ceil_div(img_w, tile_size), th = ceil_div(img_h, tile_size);
+  // xyd is not needed for counting; pass the aabb pointer as a dummy centre array
+  return tiles_count(static_cast<cudaStream_t>(stream), num_pnt, pnt2pixaabb, pnt2pixaabb, nullptr, tw, th,
+                     tile_size, workspace, workspace_bytes, num_pairs);
+}
+
+int dsplat_gauss_tile2idx_idx2pnt(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxydepth,
+                                  const float* pnt2pixaabb, uint32_t img_w, uint32_t img_h, uint32_t tile_size,
+                                  uint32_t* tile2idx, uint32_t* idx2pnt, uint64_t capacity, uint64_t* idx2tiledepth,
+                                  void* workspace, size_t workspace_bytes) {
+  if (!ts_ok(tile_size)) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
+  if (num_pnt > 0 && (!pnt2pixaabb || !pnt2pixxydepth)) return fail(DSPLAT_ERR_INVALID_ARG, "null input");
+  const uint32_t tw = ceil_div(img_w, tile_size), th = ceil_div(img_h, tile_size);
+  return tiles_fill(static_cast<cudaStream_t>(stream), num_pnt, pnt2pixxydepth, pnt2pixaabb, nullptr, int(img_w),
+                    int(img_h), tw, th, tile_size, tile2idx, idx2pnt, capacity, idx2tiledepth, workspace,
+                    workspace_bytes);
+}
+
+int dsplat_gauss_rasterize_pnt2splat2(dsplat_stream stream, uint32_t img_w, uint32_t img_h, float* pix2rgb,
+                                      const float* pnt2pixxydepth, const float* pnt2pixconvinv,
+                                      const float* pnt2pixaabb, const float* pnt2opacity, const float* pnt2rgb,
+                                      uint32_t tile_size, const uint32_t* tile2idx, const uint32_t* idx2pnt,
+                                      float* pix2transmit, uint32_t* pix2stop) {
+  if (!ts_ok(tile_size)) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
+  if (img_w == 0 || img_h == 0) return DSPLAT_OK;
+  if (!pix2rgb || !tile2idx) return fail(DSPLAT_ERR_INVALID_ARG, "null pointer");
+  TRY_CUDA(raster_fwd_aos(static_cast<cudaStream_t>(stream), int(tile_size), int(img_w), int(img_h), pix2rgb,
+                          pnt2pixxydepth, pnt2pixconvinv, pnt2pixaabb, pnt2opacity, pnt2rgb, tile2idx, idx2pnt,
+                          pix2transmit, pix2stop),
+           "raster_fwd_aos");
+  return DSPLAT_OK;
+}
+
+int dsplat_circle_pnt2splat3_to_pnt2splat2(dsplat_stream stream, uint32_t num_pnt, const float* pnt2xyz,
+                                           float* pnt2pixxydepth, float* pnt2pixrad,
+                                           const float* transform_world2ndc, uint32_t img_w, uint32_t img_h,
+                                           float radius) {
+  if (num_pnt == 0) return DSPLAT_OK;
+  if (!pnt2xyz || !pnt2pixxydepth || !pnt2pixrad || !transform_world2ndc)
+    return fail(DSPLAT_ERR_INVALID_ARG, "null pointer");
+  k_circle_project_ref<<<blocks_for(num_pnt, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      num_pnt, pnt2xyz, transform_world2ndc, int(img_w), int(img_h), radius, pnt2pixxydepth, pnt2pixrad); count_launch();
+  TRY_CUDA(cudaGetLastError(), "k_circle_project_ref");
+  return DSPLAT_OK;
+}
+
+int dsplat_circle_tile2idx_count(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxydepth,
+                                 const float* pnt2pixrad, uint32_t tile_w, uint32_t tile_h, uint32_t tile_size,
+                                 void* workspace, size_t workspace_bytes, uint64_t* num_pairs) {
+  if (num_pnt > 0 && (!pnt2pixxydepth || !pnt2pixrad)) return fail(DSPLAT_ERR_INVALID_ARG, "null input");
+  return tiles_count(static_cast<cudaStream_t>(stream), num_pnt, pnt2pixxydepth, nullptr, pnt2pixrad, tile_w, tile_h,
+                     tile_size, workspace, workspace_bytes, num_pairs);
+}
+
+int dsplat_circle_tile2idx_idx2pnt(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxydepth,
+                                   const float* pnt2pixrad, uint32_t tile_w, uint32_t tile_h, uint32_t tile_size,
+                                   uint32_t* tile2idx, uint32_t* idx2pnt, uint64_t capacity,
+                                   uint64_t* idx2tiledepth, void* workspace, size_t workspace_bytes) {
+  if (num_pnt > 0 && (!pnt2pixxydepth || !pnt2pixrad)) return fail(DSPLAT_ERR_INVALID_ARG, "null input");
+  return tiles_fill(static_cast<cudaStream_t>(stream), num_pnt, pnt2pixxydepth, nullptr, pnt2pixrad,
+                    int(tile_w * tile_size), int(tile_h * tile_size), tile_w, tile_h, tile_size, tile2idx, idx2pnt,
+                    capacity, idx2tiledepth, workspace, workspace_bytes);
+}
+
+int dsplat_circle_splat(dsplat_stream stream, uint32_t img_w, uint32_t img_h, float* pix2rgb,
+                        const float* pnt2pixxydepth, const float* pnt2pixrad, const float* pnt2rgb,
+                        uint32_t tile_size, const uint32_t* tile2idx, const uint32_t* idx2pnt) {
+  if (!ts_ok(tile_size)) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
+  if (img_w == 0 || img_h == 0) return DSPLAT_OK;
+  if (!pix2rgb || !tile2idx) return fail(DSPLAT_ERR_INVALID_ARG, "null pointer");
+  TRY_CUDA(circle_splat_tiles(static_cast<cudaStream_t>(stream), int(tile_size), int(img_w), int(img_h), pix2rgb,
+                              pnt2pixxydepth, pnt2pixrad, pnt2rgb, tile2idx, idx2pnt),
+           "circle_splat_tiles");
+  return DSPLAT_OK;
+}
+
+int dsplat_circle_splat_zbuffer(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxydepth,
+                                const float* pnt2pixrad, const void* colors, int32_t color_kind, void* pix,
+                                int32_t* pix2winner, uint32_t img_w, uint32_t img_h, uint32_t tile_size,
+                                uint64_t* zbuf) {
+  if (!ts_ok(tile_size)) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
+  if (color_kind != 0 && color_kind != 1) return fail(DSPLAT_ERR_INVALID_ARG, "color_kind must be 0 or 1");
+  const size_t npix = size_t(img_w) * img_h;
+  if (npix == 0) return DSPLAT_OK;
+  if (!zbuf || (num_pnt > 0 && (!pnt2pixxydepth || !pnt2pixrad)) || (pix && !colors))
+    return fail(DSPLAT_ERR_INVALID_ARG, "null pointer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_fill_u64<<<blocks_for(npix, 256), 256, 0, st>>>(zbuf, npix, ~0ull); count_launch();
+  if (num_pnt > 0)
+    k_circle_zbuf<<<blocks_for(num_pnt, 128), 128, 0, st>>>(num_pnt, pnt2pixxydepth, pnt2pixrad, int(img_w),
+                                                           int(img_h), int(tile_size), zbuf); count_launch();
+  k_circle_resolve<<<blocks_for(npix, 256), 256, 0, st>>>(npix, zbuf, colors, color_kind, pix, pix2winner); count_launch();
+  TRY_CUDA(cudaGetLastError(), "circle zbuffer");
+  return DSPLAT_OK;
+}
+
+int dsplat_point_rasterize_pix_zbuffer(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxyndcz,
+                                       const float* pnt2rgb, float* pix2rgb, float* pix2unitdepth,
+                                       int32_t* pix2winner, uint32_t img_w, uint32_t img_h, uint64_t* zbuf) {
+  const size_t npix = size_t(img_w) * img_h;
+  if (npix == 0) return DSPLAT_OK;
+  if (!zbuf || (num_pnt > 0 && !pnt2pixxyndcz) || (pix2rgb && !pnt2rgb))
+    return fail(DSPLAT_ERR_INVALID_ARG, "null pointer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_fill_u64<<<blocks_for(npix, 256), 256, 0, st>>>(zbuf, npix, ~0ull); count_launch();
+  if (num_pnt > 0)
+    k_point_zbuf<<<blocks_for(num_pnt, 256), 256, 0, st>>>(num_pnt, pnt2pixxyndcz, int(img_w), int(img_h), zbuf); count_launch();
+  k_point_resolve<<<blocks_for(npix, 256), 256, 0, st>>>(npix, zbuf, pnt2pixxyndcz, pnt2rgb, pix2rgb, pix2unitdepth,
+                                                         pix2winner); count_launch();
+  TRY_CUDA(cudaGetLastError(), "point zbuffer");
+  return DSPLAT_OK;
+}
+
+int dsplat_point_rasterize_pix(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxyndcz,
+                               const float* pnt2rgb, float* pix2rgb, uint32_t img_w, uint32_t img_h, uint64_t* zbuf) {
+  return dsplat_point_rasterize_pix_zbuffer(stream, num_pnt, pnt2pixxyndcz, pnt2rgb, pix2rgb, nullptr, nullptr,
+                                            img_w, img_h, zbuf);
+}
+
+int dsplat_gauss_batch_layout(int64_t num_pnt, int32_t num_views, const dsplat_view* views, int32_t tile_size,
+                              uint64_t pair_capacity, dsplat_batch_layout* out) {
+  if (!out) return fail(DSPLAT_ERR_INVALID_ARG, "out is null");
+  ViewBatch b;
+  int rc = make_batch(num_pnt, num_views, views, tile_size, &b);
+  if (rc) return rc;
+  *out = carve_batch(nullptr, uint32_t(num_pnt), b, pair_capacity).L;
+  return DSPLAT_OK;
+}
+
+int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* params, int32_t num_views,
+                               const dsplat_view* views, int32_t tile_size, uint64_t pair_capacity, void* workspace,
+                               size_t workspace_bytes, float* out_rgb, float* out_alpha, const float* target) {
+  int rc = check_params(params);
+  if (rc) return rc;
+  ViewBatch b;
+  rc = make_batch(params->num_pnt, num_views, views, tile_size, &b);
+  if (rc) return rc;
+  if (pair_capacity > 0xfffff000ull) return fail(DSPLAT_ERR_INVALID_ARG, "pair_capacity must fit in u32");
+  const uint32_t n = uint32_t(params->num_pnt);
+  BatchWs w = carve_batch(nullptr, n, b, pair_capacity);
+  if (!workspace || workspace_bytes < w.L.total_bytes) return fail(DSPLAT_ERR_WORKSPACE, "workspace too small");
+  if (!out_rgb) return fail(DSPLAT_ERR_INVALID_ARG, "out_rgb is null");
+  w = carve_batch(workspace, n, b, pair_capacity);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const uint32_t V = uint32_t(num_views), npad = w.L.npad;
+  const size_t Vp = size_t(V) * npad;
+  stage_mark(st, 0);
+  TRY_CUDA(cudaMemsetAsync(w.flags, 0, 16 * sizeof(uint32_t), st), "memset");
+  if (n == 0 || pair_capacity == 0) {
+    TRY_CUDA(cudaMemsetAsync(w.item_start, 0, (size_t(b.num_items) + 1) * 4, st), "memset");
+  } else {
+    k_iota_pad<<<blocks_for(Vp, 256), 256, 0, st>>>(w.dva, w.dka, n, npad, V); count_launch();
+    k_fused_project<<<blocks_for(n, 128), 128, 0, st>>>(n, npad, params->sh_degree, params->means,
+                                                        params->log_scales, params->quats, params->opacity,
+                                                        params->colors, b, w.rec, w.rect, w.dka, w.cnt); count_launch();
+    stage_mark(st, 1);
+    bool in_b = false;
+    TRY_CUDA(radix_sort(st, w.dka, w.dva, w.dkb, w.dvb, Vp, nullptr, 32, V, w.hist, w.scan_tmp, &in_b), "depth sort");
+    stage_mark(st, 2);
+    const uint32_t* order = in_b ? w.dvb : w.dva;
+    k_gather_counts<<<blocks_for(Vp + 1, 256), 256, 0, st>>>(order, w.cnt, n, npad, V, w.cs); count_launch();
+    TRY_CUDA(exclusive_scan(st, w.cs, w.off, Vp + 1, w.scan_tmp), "scan");
+    k_copy_total<<<1, 32, 0, st>>>(w.off, Vp, w.flags + 1); count_launch();
+    k_emit_pairs<<<blocks_for(Vp, 256), 256, 0, st>>>(order, w.cs, w.off, w.rect, n, npad, V, b, pair_capacity, w.pka,
+                                                      w.pva, w.flags); count_launch();
+    stage_mark(st, 3);
+    TRY_CUDA(radix_sort(st, w.pka, w.pva, w.pkb, w.pvb, pair_capacity, w.flags + 1, int(w.L.tile_sort_bits), 1,
+                        w.hist, w.scan_tmp, &in_b),
+             "tile sort");
+    const uint32_t* skeys = in_b ? w.pkb : w.pka;
+    k_item_ranges<<<1184, 256, 0, st>>>(skeys, w.flags + 1, pair_capacity,
+                                                                      b.num_items, w.item_start); count_launch();
+  }
+  stage_mark(st, 4);
+  const uint32_t* idx2pnt = w.pairs_in_b ? w.pvb : w.pva;
+  TRY_CUDA(raster_fwd(st, b, n, w.rec, w.item_start, idx2pnt, w.flags + 2, out_rgb, w.pix_T, w.pix_stop, target,
+                      w.grad_pix, w.item_loss),
+           "raster_fwd");
+  stage_mark(st, 5);
+  if (out_alpha) k_one_minus<<<blocks_for(b.num_pix, 256), 256, 0, st>>>(w.pix_T, out_alpha, b.num_pix); count_launch();
+  TRY_CUDA(cudaGetLastError(), "forward");
+  return DSPLAT_OK;
+}
+
+int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params* params, int32_t num_views,
+                                const dsplat_view* views, int32_t tile_size, uint64_t pair_capacity, void* workspace,
+                                size_t workspace_bytes, const float* grad_rgb, const dsplat_gauss_grads* grads) {
+  int rc = check_params(params);
+  if (rc) return rc;
+  if (!grads || (params->num_pnt > 0 && (!grads->means || !grads->log_scales || !grads->quats || !grads->opacity ||
+                                         !grads->colors)))
+    return fail(DSPLAT_ERR_INVALID_ARG, "null gradient pointer");
+  ViewBatch b;
+  rc = make_batch(params->num_pnt, num_views, views, tile_size, &b);
+  if (rc) return rc;
+  const uint32_t n = uint32_t(params->num_pnt);
+  BatchWs w = carve_batch(nullptr, n, b, pair_capacity);
+  if (!workspace || workspace_bytes < w.L.total_bytes) return fail(DSPLAT_ERR_WORKSPACE, "workspace too small");
+  w = carve_batch(workspace, n, b, pair_capacity);
+  if (n == 0) return DSPLAT_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t VN = size_t(num_views) * n;
+  stage_mark(st, 6);
+  TRY_CUDA(cudaMemsetAsync(w.grad2d, 0, 3 * VN * sizeof(float4), st), "memset");
+  TRY_CUDA(cudaMemsetAsync(w.flags + 3, 0, sizeof(uint32_t), st), "memset");
+  stage_mark(st, 7);
+  const uint32_t* idx2pnt = w.pairs_in_b ? w.pvb : w.pva;
+  TRY_CUDA(raster_bwd(st, b, n, w.rec, w.item_start, idx2pnt, w.flags + 3, grad_rgb ? grad_rgb : w.grad_pix, w.pix_T,
+                      w.pix_stop, w.grad2d),
+           "raster_bwd");
+  stage_mark(st, 8);
+  k_project_bwd<<<blocks_for(n, 128), 128, 0, st>>>(n, params->sh_degree, params->means, params->log_scales,
+                                                    params->quats, params->colors, b, w.grad2d, grads->means,
+                                                    grads->log_scales, grads->quats, grads->opacity, grads->colors); count_launch();
+  stage_mark(st, 9);
+  TRY_CUDA(cudaGetLastError(), "backward");
+  return DSPLAT_OK;
+}
+
+int dsplat_gauss_batch_status(dsplat_stream stream, const void* workspace, uint32_t* flags, uint64_t* num_pairs) {
+  if (!workspace) return fail(DSPLAT_ERR_INVALID_ARG, "workspace is null");
+  uint32_t h[2] = {0, 0};
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  TRY_CUDA(cudaMemcpyAsync(h, workspace, sizeof(h), cudaMemcpyDeviceToHost, st), "memcpy");
+  TRY_CUDA(cudaStreamSynchronize(st), "sync");
+  if (flags) *flags = h[0];
+  if (num_pairs) *num_pairs = h[1];
+  return (h[0] & kFlagPairOverflow) ? DSPLAT_ERR_CAPACITY : DSPLAT_OK;
+}
+
+int dsplat_adam_step(dsplat_stream stream, int64_t n, float* param, const float* grad, float* exp_avg,
+                     float* exp_avg_sq, float lr, float beta1, float beta2, float eps, int32_t step) {
+  if (n <= 0) return DSPLAT_OK;
+  if (!param || !grad || !exp_avg || !exp_avg_sq || step < 1) return fail(DSPLAT_ERR_INVALID_ARG, "bad argument");
+  const float bc1 = 1.f - powf(beta1, float(step)), bc2 = 1.f - powf(beta2, float(step));
+  k_adam<<<blocks_for(size_t(n), 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      size_t(n), param, grad, exp_avg, exp_avg_sq, lr, beta1, beta2, eps, bc1, bc2); count_launch();
+  TRY_CUDA(cudaGetLastError(), "adam");
+  return DSPLAT_OK;
+}
+
+}  // extern "C"
+
+extern "C" uint64_t dsplat_launch_count(void) { return dsplat::g_launches.load(); }
+
+extern "C" int dsplat_set_stage_events(void* const* events, int32_t count) {
+  if (count < 0 || count > 16 || (count > 0 && !events)) return fail(DSPLAT_ERR_INVALID_ARG, "bad event list");
+  for (int k = 0; k < count; ++k) g_stage_ev[k] = static_cast<cudaEvent_t>(events[k]);
+  g_stage_n = count;
+  return DSPLAT_OK;
+}

@@ -1,0 +1,131 @@
+// common.cuh -- shared device helpers for the del-splat B200 kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dsplat.h"
+
+#include <atomic>
+
+#define DSPLAT_MAX_VIEWS 32
+#define DSPLAT_SB_TILES 8  // unused by the LSD pipeline; kept for layout docs
+
+namespace dsplat {
+
+// Host-side count of kernel launches issued by this library (dsplat_launch_count).
+inline std::atomic<uint64_t> g_launches{0};
+inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// ---------------------------------------------------------------------------
+// Per-view constants, passed to kernels by value (<= 32 views, ~3 KB).
+// ---------------------------------------------------------------------------
+struct ViewDev {
+  float mvp[16];   // column-major world -> NDC
+  float campos[3];
+  int32_t w, h;
+  int32_t tile_w, tile_h;
+  uint32_t item_base;  // first global (view, tile) item of this view
+  uint32_t pix_base;   // first pixel of this view in the concatenated images
+  int32_t pad;
+};
+
+struct ViewBatch {
+  int32_t num_views;
+  int32_t ts;          // tile size in pixels (8, 16 or 32)
+  uint32_t num_items;  // sum of tile counts
+  uint32_t num_pix;    // sum of pixel counts
+  ViewDev v[DSPLAT_MAX_VIEWS];
+};
+
+__device__ __forceinline__ int view_of_item(const ViewBatch& b, uint32_t item) {
+  int v = 0;
+#pragma unroll 1
+  for (int k = 1; k < b.num_views; ++k)
+    if (item >= b.v[k].item_base) v = k;
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Non-contracted IEEE single-precision arithmetic.  The stages whose results
+// are compared bit-for-bit with the CPU oracle use these (or are compiled
+// with -fmad=false) so that no multiply-add is fused.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+
+// Deterministic exp(x): Cody-Waite reduction x = n*ln2 + r with ln2 split in
+// a high part that has 9 trailing zero bits (so n*LN2_HI is exact for
+// |n| < 512) and a low part, then the degree-7 Taylor polynomial of e^r on
+// |r| <= ln2/2 (truncation error < 6e-9 relative) and an exact 2^n scaling.
+// Only IEEE-exact operations are used, so the CPU oracle reproduces every
+// bit.  Results below 2^-126 flush to zero.
+__device__ __forceinline__ float dexp(float x) {
+  if (x != x) return x;
+  if (x < -87.0f) return 0.0f;
+  if (x > 88.5f) return __int_as_float(0x7f800000);
+  const float n = rintf(fm(x, 1.44269502162933349609375f));
+  float r = fs(x, fm(n, 0.693145751953125f));
+  r = fs(r, fm(n, 1.428606765330187045e-06f));
+  float p = 1.984126984126984e-04f;  // 1/5040
+  p = fa(fm(p, r), 1.388888888888889e-03f);  // 1/720
+  p = fa(fm(p, r), 8.333333333333333e-03f);  // 1/120
+  p = fa(fm(p, r), 4.166666666666667e-02f);  // 1/24
+  p = fa(fm(p, r), 1.666666666666667e-01f);  // 1/6
+  p = fa(fm(p, r), 0.5f);
+  p = fa(fm(p, r), 1.0f);
+  p = fa(fm(p, r), 1.0f);
+  const int ni = (int)n;
+  if (ni < -126) return 0.0f;
+  return fm(p, __int_as_float((ni + 127) << 23));
+}
+
+// splat_gauss.cu:105 `alpha_sum > 0.999` is a double comparison; for a float
+// alpha_sum it is exactly `alpha_sum >= 0.999f`.
+constexpr float kAlphaBreak = 0.999f;
+
+// tile_acceleration.h:43-46
+__device__ __forceinline__ uint32_t depth_bits(float ndcz) {
+  float zp1 = fa(ndcz, 1.f);
+  if (zp1 <= 0.f) zp1 = 0.f;
+  return __float_as_uint(zp1);
+}
+
+// tile_acceleration.h:22-31: [floor(min/ts), floor(max/ts)+1) clipped to the
+// tile grid.  Out-of-range and NaN values clamp instead of overflowing.
+__device__ __forceinline__ int tile_lo(float a, float tsf, int lim) {
+  const float f = floorf(__fdiv_rn(a, tsf));
+  return (f >= 0.f) ? (f < float(lim) ? int(f) : lim) : 0;
+}
+__device__ __forceinline__ int tile_hi(float a, float tsf, int lim) {
+  const float f = floorf(__fdiv_rn(a, tsf));
+  return (f >= 0.f) ? (f < float(lim) ? int(f) + 1 : lim) : 0;
+}
+
+// rect packing: x0 | y0 << 16 in .x, x1 | y1 << 16 in .y
+__device__ __forceinline__ uint2 pack_rect(int x0, int y0, int x1, int y1) {
+  return make_uint2(uint32_t(x0) | (uint32_t(y0) << 16),
+                    uint32_t(x1) | (uint32_t(y1) << 16));
+}
+
+// ---------------------------------------------------------------------------
+// Error flag (device) -- kernels record the first failure and return.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void set_flag(uint32_t* flags, uint32_t bit) {
+  atomicOr(flags, bit);
+}
+constexpr uint32_t kFlagPairOverflow = 1u;
+
+}  // namespace dsplat
+
+#define DSPLAT_CUDA_TRY(expr)                       \
+  do {                                              \
+    cudaError_t _e = (expr);                        \
+    if (_e != cudaSuccess) return dsplat::map_err(_e); \
+  } while (0)
+
+namespace dsplat {
+inline int map_err(cudaError_t e) {
+  return e == cudaSuccess ? DSPLAT_OK : DSPLAT_ERR_CUDA;
+}
+}  // namespace dsplat

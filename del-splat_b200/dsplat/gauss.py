@@ -1,0 +1,215 @@
+"""Torch-facing wrappers of the batched Gaussian pipeline (C ABI in dsplat.h).
+
+``GaussBatch`` owns one workspace for a fixed list of cameras and drives
+``dsplat_gauss_batch_forward`` / ``_backward``.  ``render`` is the
+differentiable entry point (a ``torch.autograd.Function``).  Torch is used
+for device memory and the current stream only; every stage runs in
+libdsplat.so.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .scenes import Camera
+
+PARAM_NAMES = ("means", "log_scales", "quats", "opacity", "colors")
+
+
+def _stream_ptr(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _require_cuda(t: torch.Tensor, name: str) -> None:
+    if not t.is_cuda:
+        raise RuntimeError(f"{name}: del-splat-b200 runs on CUDA devices only (got {t.device})")
+    if t.dtype != torch.float32:
+        raise TypeError(f"{name}: expected float32, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name}: expected a contiguous tensor")
+
+
+def make_views(cameras: Sequence[Camera]):
+    arr = (N.View * len(cameras))()
+    for i, c in enumerate(cameras):
+        arr[i].mvp[:] = [float(x) for x in np.asarray(c.mvp, np.float32).reshape(16)]
+        arr[i].campos[:] = [float(x) for x in np.asarray(c.campos, np.float32).reshape(3)]
+        arr[i].width = int(c.width)
+        arr[i].height = int(c.height)
+    return arr
+
+
+def params_struct(p: Dict[str, torch.Tensor], sh_degree: int) -> N.GaussParams:
+    for k in PARAM_NAMES:
+        _require_cuda(p[k], k)
+    n = p["means"].shape[0]
+    return N.GaussParams(n, sh_degree, p["means"].data_ptr(), p["log_scales"].data_ptr(), p["quats"].data_ptr(),
+                         p["opacity"].data_ptr(), p["colors"].data_ptr())
+
+
+class GaussBatch:
+    """Workspace + launches for rendering N Gaussians into a fixed set of views.
+
+    The forward state (tile lists, stop positions, transmittance) lives in the
+    workspace until the next forward; ``backward`` uses the latest forward.
+    """
+
+    def __init__(self, num_pnt: int, cameras: Sequence[Camera], tile_size: int = 16, sh_degree: int = 3,
+                 pair_capacity: int = 1 << 20, device: Optional[torch.device] = None):
+        self.device = torch.device(device or "cuda")
+        self.n = int(num_pnt)
+        self.cameras = list(cameras)
+        self.tile_size = int(tile_size)
+        self.sh_degree = int(sh_degree)
+        self.views = make_views(self.cameras)
+        self.num_views = len(self.cameras)
+        self.pix_offsets = np.cumsum([0] + [c.width * c.height for c in self.cameras]).tolist()
+        self._alloc(int(pair_capacity))
+
+    # ----------------------------------------------------------- workspace
+    def _alloc(self, capacity: int) -> None:
+        self.capacity = max(1, capacity)
+        L = N.BatchLayout()
+        N.check(N.lib().dsplat_gauss_batch_layout(self.n, self.num_views, self.views, self.tile_size,
+                                                  self.capacity, ctypes.byref(L)), "batch_layout")
+        self.layout = L
+        self.ws = torch.empty(int(L.total_bytes), dtype=torch.uint8, device=self.device)
+        self.out_rgb = torch.empty(int(L.num_pix) * 3, dtype=torch.float32, device=self.device)
+
+    def ensure_capacity(self, params: Dict[str, torch.Tensor], slack: float = 1.05) -> int:
+        """Run one forward, read the pair total and grow the pair buffers."""
+        self.forward(params)
+        flags, pairs = self.status()
+        if pairs > self.capacity:
+            self._alloc(int(pairs * slack) + 1024)
+            self.forward(params)
+            flags, pairs = self.status()
+            if flags:
+                raise RuntimeError("pair capacity still exceeded after resize")
+        return pairs
+
+    def status(self):
+        f = N.c_u32(0)
+        p = N.c_u64(0)
+        N.lib().dsplat_gauss_batch_status(_stream_ptr(self.device), self.ws.data_ptr(), ctypes.byref(f),
+                                          ctypes.byref(p))
+        return int(f.value), int(p.value)
+
+    # ----------------------------------------------------------- launches
+    def forward(self, params: Dict[str, torch.Tensor], target: Optional[torch.Tensor] = None,
+                out_alpha: Optional[torch.Tensor] = None, out_rgb: Optional[torch.Tensor] = None) -> torch.Tensor:
+        ps = params_struct(params, self.sh_degree)
+        out = self.out_rgb if out_rgb is None else out_rgb
+        if target is not None:
+            _require_cuda(target, "target")
+        N.check(N.lib().dsplat_gauss_batch_forward(
+            _stream_ptr(self.device), ctypes.byref(ps), self.num_views, self.views, self.tile_size, self.capacity,
+            self.ws.data_ptr(), self.ws.numel(), out.data_ptr(),
+            out_alpha.data_ptr() if out_alpha is not None else None,
+            target.data_ptr() if target is not None else None), "batch_forward")
+        return out
+
+    def backward(self, params: Dict[str, torch.Tensor], grads: Dict[str, torch.Tensor],
+                 grad_rgb: Optional[torch.Tensor] = None) -> None:
+        ps = params_struct(params, self.sh_degree)
+        for k in PARAM_NAMES:
+            _require_cuda(grads[k], "grad " + k)
+        gs = N.GaussGrads(grads["means"].data_ptr(), grads["log_scales"].data_ptr(), grads["quats"].data_ptr(),
+                          grads["opacity"].data_ptr(), grads["colors"].data_ptr())
+        if grad_rgb is not None:
+            _require_cuda(grad_rgb, "grad_rgb")
+        N.check(N.lib().dsplat_gauss_batch_backward(
+            _stream_ptr(self.device), ctypes.byref(ps), self.num_views, self.views, self.tile_size, self.capacity,
+            self.ws.data_ptr(), self.ws.numel(), grad_rgb.data_ptr() if grad_rgb is not None else None,
+            ctypes.byref(gs)), "batch_backward")
+
+    # ----------------------------------------------------------- views of the workspace
+    def _ws(self, off: int, count: int, dtype: torch.dtype) -> torch.Tensor:
+        itemsize = torch.empty((), dtype=dtype).element_size()
+        return self.ws[off: off + count * itemsize].view(dtype)
+
+    def images(self, flat: Optional[torch.Tensor] = None) -> List[torch.Tensor]:
+        flat = self.out_rgb if flat is None else flat
+        out = []
+        for v, c in enumerate(self.cameras):
+            a, b = self.pix_offsets[v], self.pix_offsets[v + 1]
+            out.append(flat[3 * a: 3 * b].view(c.height, c.width, 3))
+        return out
+
+    def per_pixel(self, name: str) -> List[torch.Tensor]:
+        L = self.layout
+        off = {"T": L.off_pix_T, "stop": L.off_pix_stop}[name]
+        dt = torch.float32 if name == "T" else torch.int32
+        flat = self._ws(off, int(L.num_pix), dt)
+        return [flat[self.pix_offsets[v]: self.pix_offsets[v + 1]].view(c.height, c.width)
+                for v, c in enumerate(self.cameras)]
+
+    def tile_lists(self, view: int):
+        """(tile2idx [T+1], idx2pnt [P_v]) of one view, in the reference's format."""
+        L = self.layout
+        ts = self.tile_size
+        item_base = 0
+        for v in range(view):
+            c = self.cameras[v]
+            item_base += ((c.width + ts - 1) // ts) * ((c.height + ts - 1) // ts)
+        c = self.cameras[view]
+        T = ((c.width + ts - 1) // ts) * ((c.height + ts - 1) // ts)
+        starts = self._ws(L.off_item_start, int(L.num_items) + 1, torch.int32)
+        s = starts[item_base: item_base + T + 1].to(torch.int64)
+        idx = self._ws(L.off_idx2pnt, self.capacity, torch.int32)
+        p0, p1 = int(s[0]), int(s[-1])
+        return (s - p0).to(torch.int32), idx[p0:p1]
+
+    def item_loss(self) -> torch.Tensor:
+        return self._ws(self.layout.off_item_loss, int(self.layout.num_items), torch.float32)
+
+    def grad2d(self) -> torch.Tensor:
+        return self._ws(self.layout.off_grad2d, self.num_views * self.n * 12, torch.float32).view(
+            self.num_views, self.n, 12)
+
+    def records(self) -> torch.Tensor:
+        return self._ws(self.layout.off_rec, self.num_views * self.n * 12, torch.float32).view(
+            self.num_views, self.n, 12)
+
+
+class _RenderFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, means, log_scales, quats, opacity, colors, batch: GaussBatch):
+        params = dict(means=means.detach(), log_scales=log_scales.detach(), quats=quats.detach(),
+                      opacity=opacity.detach(), colors=colors.detach())
+        out = torch.empty(int(batch.layout.num_pix) * 3, dtype=torch.float32, device=means.device)
+        batch.forward(params, out_rgb=out)
+        ctx.batch = batch
+        ctx.save_for_backward(means, log_scales, quats, opacity, colors)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_rgb):
+        means, log_scales, quats, opacity, colors = ctx.saved_tensors
+        params = dict(means=means.detach(), log_scales=log_scales.detach(), quats=quats.detach(),
+                      opacity=opacity.detach(), colors=colors.detach())
+        grads = {k: torch.zeros_like(v) for k, v in params.items()}
+        ctx.batch.backward(params, grads, grad_rgb.contiguous())
+        return grads["means"], grads["log_scales"], grads["quats"], grads["opacity"], grads["colors"], None
+
+
+def render(means, log_scales, quats, opacity, colors, batch: GaussBatch) -> List[torch.Tensor]:
+    """Differentiable render of all views of ``batch``; returns [H,W,3] images.
+
+    The backward of the returned images runs the hand-written backward
+    rasteriser and projection backward.  Call backward before the next render
+    on the same batch (the forward state lives in its workspace).
+    """
+    flat = _RenderFn.apply(means, log_scales, quats, opacity, colors, batch)
+    return batch.images(flat)
+
+
+def adam_step(param: torch.Tensor, grad: torch.Tensor, exp_avg: torch.Tensor, exp_avg_sq: torch.Tensor,
+              lr: float, beta1: float, beta2: float, eps: float, step: int) -> None:
+    N.check(N.lib().dsplat_adam_step(_stream_ptr(param.device), param.numel(), param.data_ptr(), grad.data_ptr(),
+                                     exp_avg.data_ptr(), exp_avg_sq.data_ptr(), lr, beta1, beta2, eps, step),
+            "adam_step")

@@ -1,0 +1,220 @@
+/*
+ * dsplat.h -- C ABI of the B200 splatting library (libdsplat.so).
+ *
+ * Plain C: device pointers, sizes and a cudaStream_t (passed as void*).
+ * Every call is asynchronous on the given stream unless it says otherwise,
+ * returns a status code and never aborts.  The library allocates no device
+ * memory: outputs and workspaces belong to the caller (size them with the
+ * *_workspace_size queries).  Thread-safe as long as two calls do not share a
+ * workspace at the same time.
+ *
+ * Each entry point cites the del-splat (nobuyuki83/del-splat) interface it
+ * replaces.  Array conventions follow the reference:
+ *   pnt2xyz [N,3], pnt2quat [N,4] (x,y,z,w), pnt2scale [N,3] (std-dev),
+ *   transform_world2ndc [16] column-major (larger ndc_z = nearer),
+ *   pnt2pixxydepth [N,3] (pixel x, pixel y, ndc z), pnt2pixconvinv [N,3]
+ *   (conic a,b,c), pnt2pixaabb [N,4] (xmin,ymin,xmax,ymax),
+ *   tile2idx [T+1] u32, idx2pnt [P] u32, pix2rgb [H,W,3] f32.
+ */
+#ifndef DSPLAT_H
+#define DSPLAT_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSPLAT_OK 0
+#define DSPLAT_ERR_INVALID_ARG 1  /* null pointer, bad size or shape     */
+#define DSPLAT_ERR_CAPACITY 2     /* pair buffer too small (see *_status) */
+#define DSPLAT_ERR_CUDA 3         /* a CUDA runtime call failed           */
+#define DSPLAT_ERR_WORKSPACE 4    /* workspace smaller than required      */
+#define DSPLAT_ERR_UNSUPPORTED 5  /* e.g. tile size other than 8/16/32    */
+
+typedef void* dsplat_stream; /* cudaStream_t */
+
+/* Library version string and the message of the last failed call on this
+ * host thread. */
+const char* dsplat_version(void);
+const char* dsplat_last_error(void);
+/* Number of kernel launches this library has issued in the process. */
+uint64_t dsplat_launch_count(void);
+
+/* ===================== del-splat-cudarc :: splat_gauss ================== */
+
+/* del-splat-cudarc/src/splat_gauss.rs:6-44 pnt2splat3_to_pnt2splat2
+ * (kernel splat_gauss.cu:10-53). */
+int dsplat_gauss_pnt2splat3_to_pnt2splat2(dsplat_stream stream, uint32_t num_pnt, const float* pnt2xyz,
+                                          const float* pnt2scale, const float* pnt2quat, float* pnt2pixxydepth,
+                                          float* pnt2pixconvinv, float* pnt2pixaabb,
+                                          const float* transform_world2ndc, uint32_t img_w, uint32_t img_h);
+
+/* Workspace for the tile2idx / idx2pnt builders below (Gaussian and circle). */
+size_t dsplat_tile2idx_workspace_size(uint32_t num_pnt, uint32_t tile_w, uint32_t tile_h, uint64_t num_pairs);
+
+/* del-splat-cudarc/src/splat_gauss.rs:96-195 tile2idx_idx2pnt, split in two
+ * because the reference allocates its outputs: (1) count -- synchronises the
+ * stream and returns the pair total P on the host, like the reference's D2H
+ * read at splat_gauss.rs:147; (2) fill caller buffers tile2idx[T+1] and
+ * idx2pnt[capacity] (capacity >= P).  idx2tiledepth (nullable) receives the
+ * sorted 64-bit keys (tile << 32 | bits(max(ndc_z+1, 0))).  Unlike the
+ * reference, the given tile_size is used throughout (the reference
+ * hard-codes 16 in its count/fill launches, splat_gauss.rs:127,176). */
+int dsplat_gauss_tile2idx_count(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixaabb, uint32_t img_w,
+                                uint32_t img_h, uint32_t tile_size, void* workspace, size_t workspace_bytes,
+                                uint64_t* num_pairs);
+int dsplat_gauss_tile2idx_idx2pnt(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxydepth,
+                                  const float* pnt2pixaabb, uint32_t img_w, uint32_t img_h, uint32_t tile_size,
+                                  uint32_t* tile2idx, uint32_t* idx2pnt, uint64_t capacity, uint64_t* idx2tiledepth,
+                                  void* workspace, size_t workspace_bytes);
+
+/* del-splat-cudarc/src/splat_gauss.rs:46-94 rasterize_pnt2splat2 (kernel
+ * splat_gauss.cu:56-109): accumulates into pix2rgb like the reference.
+ * pix2transmit [H,W] and pix2stop [H,W] (nullable) receive the final
+ * transmittance and the list position where each pixel's walk stopped. */
+int dsplat_gauss_rasterize_pnt2splat2(dsplat_stream stream, uint32_t img_w, uint32_t img_h, float* pix2rgb,
+                                      const float* pnt2pixxydepth, const float* pnt2pixconvinv,
+                                      const float* pnt2pixaabb, const float* pnt2opacity, const float* pnt2rgb,
+                                      uint32_t tile_size, const uint32_t* tile2idx, const uint32_t* idx2pnt,
+                                      float* pix2transmit, uint32_t* pix2stop);
+
+/* ===================== del-splat-cudarc :: splat_circle ================= */
+
+/* del-splat-cudarc/src/splat_circle.rs:96-132 pnt2splat3_to_pnt2splat2
+ * (kernel splat_circle.cu:7-41). */
+int dsplat_circle_pnt2splat3_to_pnt2splat2(dsplat_stream stream, uint32_t num_pnt, const float* pnt2xyz,
+                                           float* pnt2pixxydepth, float* pnt2pixrad,
+                                           const float* transform_world2ndc, uint32_t img_w, uint32_t img_h,
+                                           float radius);
+
+/* del-splat-cudarc/src/splat_circle.rs:3-94 tile2idx_idx2pnt(tile_shape, ..):
+ * same two-step contract as the Gaussian version; box = centre +- radius. */
+int dsplat_circle_tile2idx_count(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxydepth,
+                                 const float* pnt2pixrad, uint32_t tile_w, uint32_t tile_h, uint32_t tile_size,
+                                 void* workspace, size_t workspace_bytes, uint64_t* num_pairs);
+int dsplat_circle_tile2idx_idx2pnt(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxydepth,
+                                   const float* pnt2pixrad, uint32_t tile_w, uint32_t tile_h, uint32_t tile_size,
+                                   uint32_t* tile2idx, uint32_t* idx2pnt, uint64_t capacity,
+                                   uint64_t* idx2tiledepth, void* workspace, size_t workspace_bytes);
+
+/* del-splat-cudarc/src/splat_circle.rs:134-177 splat (kernel
+ * splat_circle.cu:93-132): painter over the tile lists; writes covered pixels. */
+int dsplat_circle_splat(dsplat_stream stream, uint32_t img_w, uint32_t img_h, float* pix2rgb,
+                        const float* pnt2pixxydepth, const float* pnt2pixrad, const float* pnt2rgb,
+                        uint32_t tile_size, const uint32_t* tile2idx, const uint32_t* idx2pnt);
+
+/* Circle splat through a packed 64-bit depth|index z-buffer (no tile lists);
+ * same winners as dsplat_circle_splat over tile lists of tile_size.
+ * colors: color_kind 0 -> float rgb [N,3] into pix float [H,W,3];
+ *         color_kind 1 -> u32 rgba [N] into pix u32 [H,W].
+ * zbuf: caller workspace of img_w*img_h u64.  pix2winner [H,W] nullable. */
+int dsplat_circle_splat_zbuffer(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxydepth,
+                                const float* pnt2pixrad, const void* colors, int32_t color_kind, void* pix,
+                                int32_t* pix2winner, uint32_t img_w, uint32_t img_h, uint32_t tile_size,
+                                uint64_t* zbuf);
+
+/* ===================== del-splat-dlpack :: splat_point ================== */
+
+/* del-splat-dlpack/src/splat_point.rs:47-106 point_splat_rasterize_pix_zbuffer
+ * (kernel splat_point.cu:49-74): nearest point per pixel; pix2unitdepth gets
+ * 1-(ndc_z+1)/2 of the winner or FLT_MAX; pix2rgb untouched where empty.
+ * zbuf: caller workspace of img_w*img_h u64.  pix2winner nullable. */
+int dsplat_point_rasterize_pix_zbuffer(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxyndcz,
+                                       const float* pnt2rgb, float* pix2rgb, float* pix2unitdepth,
+                                       int32_t* pix2winner, uint32_t img_w, uint32_t img_h, uint64_t* zbuf);
+
+/* del-splat-dlpack/src/splat_point.rs:12-43 point_splat_rasterize_pix (the
+ * reference has only a CPU branch, its GPU arm is todo!()). */
+int dsplat_point_rasterize_pix(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxyndcz,
+                               const float* pnt2rgb, float* pix2rgb, uint32_t img_w, uint32_t img_h, uint64_t* zbuf);
+
+/* ============ differentiable, batched Gaussian splatting (new) =========== */
+/* No reference counterpart: the reference is forward-only and one view at a
+ * time.  Parameters: means [N,3], log_scales [N,3], quats [N,4] (x,y,z,w,
+ * normalised inside), opacity [N] (used as is), colors [N,3] RGB when
+ * sh_degree < 0, else SH coefficients [N,(sh_degree+1)^2,3]. */
+typedef struct {
+  float mvp[16];    /* column-major world->NDC */
+  float campos[3];  /* camera centre, for the SH view direction */
+  int32_t width, height;
+} dsplat_view;
+
+typedef struct {
+  int64_t num_pnt;
+  int32_t sh_degree; /* -1 (RGB) or 0..3 */
+  const float* means;
+  const float* log_scales;
+  const float* quats;
+  const float* opacity;
+  const float* colors;
+} dsplat_gauss_params;
+
+typedef struct { /* gradients, accumulated (+=) */
+  float* means;
+  float* log_scales;
+  float* quats;
+  float* opacity;
+  float* colors;
+} dsplat_gauss_grads;
+
+/* Byte offsets of the batch state inside the workspace (for inspection). */
+typedef struct {
+  size_t total_bytes;
+  uint32_t num_items; /* sum over views of tiles */
+  uint32_t num_pix;   /* sum over views of pixels */
+  uint32_t npad;      /* per-view padded point count of the depth sort */
+  uint32_t tile_sort_bits;
+  size_t off_flags;      /* u32[4]: flags, total pairs, counters */
+  size_t off_rec;        /* float4[V*N*3] per-view 2D records */
+  size_t off_rect;       /* uint2[V*N] tile spans */
+  size_t off_cnt;        /* u32[V*N] tiles per point */
+  size_t off_order;      /* u32[V*npad] points in depth order per view */
+  size_t off_item_start; /* u32[num_items+1] */
+  size_t off_idx2pnt;    /* u32[capacity] points sorted by (item, depth) */
+  size_t off_item_key;   /* u32[capacity] item id of each sorted pair */
+  size_t off_pix_T;      /* f32[num_pix] final transmittance */
+  size_t off_pix_stop;   /* u32[num_pix] list position where the walk stopped */
+  size_t off_grad_pix;   /* f32[num_pix*3] dL/dpixel (loss gradient) */
+  size_t off_item_loss;  /* f32[num_items] per-item partial L2 loss */
+  size_t off_grad2d;     /* float4[V*N*3] per-view 2D gradients */
+} dsplat_batch_layout;
+
+int dsplat_gauss_batch_layout(int64_t num_pnt, int32_t num_views, const dsplat_view* views, int32_t tile_size,
+                              uint64_t pair_capacity, dsplat_batch_layout* out);
+
+/* Forward over all views: projection (+SH), depth sort, pair emission, tile
+ * sort, ranges and rasterisation in one launch sequence, no host sync (CUDA-
+ * graph capturable).  out_rgb: concatenated [H_v,W_v,3] images; out_alpha
+ * (nullable): 1 - T per pixel.  target (nullable, same layout as out_rgb):
+ * also computes the L2 loss sum (per-item partials in the workspace) and
+ * its pixel gradient for dsplat_gauss_batch_backward. */
+int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* params, int32_t num_views,
+                               const dsplat_view* views, int32_t tile_size, uint64_t pair_capacity, void* workspace,
+                               size_t workspace_bytes, float* out_rgb, float* out_alpha, const float* target);
+
+/* Backward of the last forward on this workspace.  grad_rgb (nullable):
+ * dL/d out_rgb; null uses the L2-loss gradient stored by the forward. */
+int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params* params, int32_t num_views,
+                                const dsplat_view* views, int32_t tile_size, uint64_t pair_capacity, void* workspace,
+                                size_t workspace_bytes, const float* grad_rgb, const dsplat_gauss_grads* grads);
+
+/* Synchronises the stream and reports the overflow flag and the pair total of
+ * the last forward (a capacity overflow leaves outputs undefined). */
+int dsplat_gauss_batch_status(dsplat_stream stream, const void* workspace, uint32_t* flags, uint64_t* num_pairs);
+
+/* Profiling hook: CUDA events (cudaEvent_t) recorded on the launch stream at
+ * the stage boundaries of the batched calls on this host thread:
+ * forward 0 start, 1 projected, 2 depth-sorted, 3 pairs emitted, 4 tile lists
+ * ready, 5 rasterised; backward 6 start, 7 gradients cleared, 8 backward
+ * raster done, 9 projection backward done.  count 0 disables. */
+int dsplat_set_stage_events(void* const* events, int32_t count);
+
+/* Adam (bias-corrected) on one parameter tensor, in place. */
+int dsplat_adam_step(dsplat_stream stream, int64_t n, float* param, const float* grad, float* exp_avg,
+                     float* exp_avg_sq, float lr, float beta1, float beta2, float eps, int32_t step);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DSPLAT_H */
