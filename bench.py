@@ -303,7 +303,7 @@ def main():
             params[k].copy_(host_pinned[k], non_blocking=True)
         target.copy_(tgt_pinned, non_blocking=True)
         step_batched()
-        loss_host.copy_(batch.item_loss().sum().reshape(1), non_blocking=True)
+        loss_host.copy_(batch.slab_loss().sum().reshape(1), non_blocking=True)
 
     for _ in range(args.warmup):
         step_e2e()
@@ -321,21 +321,21 @@ def main():
     # roofline of the dominant kernel (algorithmic bytes per launch / event time)
     peak, peak_kind = peaks()
     npix = int(batch.layout.num_pix)
-    names = ["project_fwd", "depth_sort", "emit_pairs", "tile_sort_ranges", "raster_fwd", "(host gap)",
+    names = ["project_fwd", "depth_sort", "tile_lists", "(unused)", "raster_fwd", "(host gap)",
              "grad_clear", "raster_bwd", "project_bwd"]
     s_sh = 48
     bytes_alg = {
         "project_fwd": base.n * (40 + 4 + 4 * s_sh) + V * base.n * (48 + 8 + 4 + 4),
         "depth_sort": 4 * V * batch.layout.npad * 16,
-        "emit_pairs": V * batch.layout.npad * 12 + pairs * 8,
-        "tile_sort_ranges": pairs * 16 * ((int(batch.layout.tile_sort_bits) + 7) // 8),
+        "(unused)": 0,
+        "tile_lists": pairs * 4 + 2 * V * batch.layout.npad * 12,
         "raster_fwd": pairs * 40 + npix * 20,
         "raster_bwd": npix * 20 + pairs * 40 + V * base.n * 36,
         "project_bwd": base.n * (40 + 4 * s_sh) + V * base.n * 48 + base.n * (40 + 4 * s_sh),
         "grad_clear": V * base.n * 48,
         "(host gap)": 0,
     }
-    dom = max((n for n in names if n != "(host gap)"), key=lambda n: stage_ms[names.index(n)])
+    dom = max((n for n in names if not n.startswith("(")), key=lambda n: stage_ms[names.index(n)])
     dom_ms = stage_ms[names.index(dom)]
     achieved = bytes_alg[dom] / (dom_ms / 1e3) / 1e9
 

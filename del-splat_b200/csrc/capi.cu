@@ -22,10 +22,14 @@ __global__ void k_project_bwd(uint32_t, int, const float*, const float*, const f
                               const float4*, float*, float*, float*, float*, float*);
 __global__ void k_adam(size_t, float*, const float*, float*, float*, float, float, float, float, float, float);
 __global__ void k_iota_pad(uint32_t*, uint32_t*, uint32_t, uint32_t, uint32_t);
-__global__ void k_gather_counts(const uint32_t*, const uint32_t*, uint32_t, uint32_t, uint32_t, uint32_t*);
-__global__ void k_emit_pairs(const uint32_t*, const uint32_t*, const uint32_t*, const uint2*, uint32_t, uint32_t,
-                             uint32_t, const ViewBatch, uint64_t, uint32_t*, uint32_t*, uint32_t*);
-__global__ void k_item_ranges(const uint32_t*, const uint32_t*, uint64_t, uint32_t, uint32_t*);
+__global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*);
+__global__ void k_sb_scatter(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
+                             uint64_t, uint32_t*, uint32_t*);
+__global__ void k_tile_count(const uint32_t*, const uint32_t*, uint32_t, uint64_t, const uint2*, uint32_t,
+                             const ViewBatch, uint32_t*);
+__global__ void k_tile_scatter(const uint32_t*, const uint32_t*, uint32_t, uint64_t, const uint2*, uint32_t,
+                               const ViewBatch, const uint32_t*, uint32_t*, uint32_t*, uint32_t*);
+__global__ void k_clamp_ranges(uint32_t*, uint32_t, uint64_t, uint32_t*);
 __global__ void k_copy_total(const uint32_t*, size_t, uint32_t*);
 __global__ void k_make_keys64(const uint32_t*, const uint32_t*, const float*, const uint32_t*, uint64_t, uint64_t*);
 __global__ void k_fill_u64(uint64_t*, size_t, uint64_t);
@@ -51,14 +55,6 @@ cudaError_t circle_splat_tiles(cudaStream_t, int, int, int, float*, const float*
 __global__ void k_one_minus(const float* __restrict__ T, float* __restrict__ out, size_t n) {
   const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) out[i] = 1.f - T[i];
-}
-
-__global__ void k_copy_u32_count(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
-                                 const uint32_t* __restrict__ count_ptr, uint64_t capacity) {
-  uint32_t cnt = *count_ptr;
-  if (cnt > capacity) cnt = uint32_t(capacity);
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < cnt; i += size_t(gridDim.x) * blockDim.x)
-    dst[i] = src[i];
 }
 
 namespace {
@@ -118,41 +114,84 @@ struct Carver {
 };
 
 // ---------------------------------------------------------------------------
+// Tile lists from rank order (shared by the drop-in and batched paths):
+// stage 1 superblock multisplit, stage 2 per-tile multisplit; see tiles.cu.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kChunk = 4096;  // ranks per stage-1 chunk (= kSortTile)
+
+struct ListsWs {
+  uint32_t *cnt1, *off1, *list1, *tcnt;
+};
+
+size_t lists_scan_words(const ViewBatch& b, uint32_t npad) {
+  const size_t a = size_t(b.num_sb) * (npad / kChunk) + 1, c = size_t(b.num_items) + 1;
+  return a > c ? a : c;
+}
+
+void carve_lists(Carver& c, const ViewBatch& b, uint32_t npad, size_t cap, ListsWs* L, size_t* off_list1) {
+  const size_t m = size_t(b.num_sb) * (npad / kChunk) + 1;
+  L->cnt1 = c.take<uint32_t>(m);
+  L->off1 = c.take<uint32_t>(m);
+  L->list1 = c.take<uint32_t>(cap, off_list1);
+  L->tcnt = c.take<uint32_t>(size_t(b.num_items) + 1);
+}
+
+int build_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npad, const uint32_t* order,
+                const uint2* rect, const ListsWs& L, uint32_t* scan_tmp, uint32_t* item_start, uint32_t* idx2pnt,
+                uint32_t* out_tile, uint64_t capacity, uint32_t* flags) {
+  const uint32_t nchunk = npad / kChunk;
+  const size_t m = size_t(b.num_sb) * nchunk;
+  const unsigned grid1 = unsigned(b.num_views) * nchunk;
+  const size_t smem1 = size_t(b.max_sb) * sizeof(uint32_t);
+  const size_t smem3 = 8 * smem1;
+  if (smem3 > 48 * 1024) {
+    if (smem3 > 200 * 1024) return fail(DSPLAT_ERR_UNSUPPORTED, "too many superblocks in one view");
+    TRY_CUDA(cudaFuncSetAttribute(k_sb_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)), "attr");
+  }
+  k_sb_count<<<grid1, 256, smem1, st>>>(order, rect, n, npad, b, L.cnt1);
+  count_launch();
+  TRY_CUDA(cudaMemsetAsync(L.cnt1 + m, 0, sizeof(uint32_t), st), "memset");
+  TRY_CUDA(exclusive_scan(st, L.cnt1, L.off1, m + 1, scan_tmp), "scan");
+  k_sb_scatter<<<grid1, 256, smem3, st>>>(order, rect, n, npad, b, L.off1, capacity, L.list1, flags);
+  count_launch();
+  TRY_CUDA(cudaMemsetAsync(L.tcnt + b.num_items, 0, sizeof(uint32_t), st), "memset");
+  k_tile_count<<<b.num_sb, 256, 0, st>>>(L.list1, L.off1, nchunk, capacity, rect, n, b, L.tcnt);
+  count_launch();
+  TRY_CUDA(exclusive_scan(st, L.tcnt, item_start, size_t(b.num_items) + 1, scan_tmp), "scan");
+  k_copy_total<<<1, 32, 0, st>>>(item_start, b.num_items, flags + 1);
+  count_launch();
+  k_tile_scatter<<<b.num_sb, 256, 0, st>>>(L.list1, L.off1, nchunk, capacity, rect, n, b, item_start, idx2pnt,
+                                           out_tile, flags);
+  count_launch();
+  k_clamp_ranges<<<64, 256, 0, st>>>(item_start, b.num_items, capacity, flags);
+  count_launch();
+  TRY_CUDA(cudaGetLastError(), "tile lists");
+  return DSPLAT_OK;
+}
+
+void fill_sb_layout(ViewBatch* b) {
+  uint32_t sb = 0, mx = 0;
+  for (int v = 0; v < b->num_views; ++v) {
+    ViewDev& d = b->v[v];
+    d.sb_base = sb;
+    const uint32_t c = uint32_t((d.tile_w + 7) / 8) * uint32_t((d.tile_h + 7) / 8);
+    sb += c;
+    mx = c > mx ? c : mx;
+  }
+  b->num_sb = sb;
+  b->max_sb = mx;
+}
+
+// ---------------------------------------------------------------------------
 // Single-view tile list builder shared by the Gaussian and circle entries.
 // ---------------------------------------------------------------------------
 struct TileWs {
   uint32_t* flags;  // [0] flags, [1] total pairs
   uint2* rect;
-  uint32_t *cnt, *dka, *dva, *dkb, *dvb, *cs, *off, *hist, *scan_tmp, *pka, *pva, *pkb;
+  uint32_t *cnt, *dka, *dva, *dkb, *dvb, *hist, *scan_tmp, *out_tile;
+  ListsWs lists;
   size_t bytes;
 };
-
-TileWs carve_tiles(void* ws, uint32_t n, uint32_t tile_w, uint32_t tile_h, uint64_t pairs) {
-  (void)tile_w;
-  (void)tile_h;
-  const uint32_t npad = ceil_div(n > 0 ? n : 1, kSortTile) * kSortTile;
-  const size_t cap = pairs > 0 ? pairs : 1;
-  Carver c(ws);
-  TileWs t;
-  t.flags = c.take<uint32_t>(16);
-  t.rect = c.take<uint2>(n + 1);
-  t.cnt = c.take<uint32_t>(size_t(n) + 1);
-  t.dka = c.take<uint32_t>(npad);
-  t.dva = c.take<uint32_t>(npad);
-  t.dkb = c.take<uint32_t>(npad);
-  t.dvb = c.take<uint32_t>(npad);
-  t.cs = c.take<uint32_t>(size_t(npad) + 1);
-  t.off = c.take<uint32_t>(size_t(npad) + 1);
-  const size_t hw = radix_hist_words(npad > cap ? npad : cap);
-  t.hist = c.take<uint32_t>(hw);
-  const size_t sw = scan_tmp_words(hw > size_t(npad) + 1 ? hw : size_t(npad) + 1);
-  t.scan_tmp = c.take<uint32_t>(sw);
-  t.pka = c.take<uint32_t>(cap);
-  t.pva = c.take<uint32_t>(cap);
-  t.pkb = c.take<uint32_t>(cap);
-  t.bytes = c.off;
-  return t;
-}
 
 ViewBatch single_view_batch(int w, int h, int ts, uint32_t tile_w, uint32_t tile_h) {
   ViewBatch b;
@@ -165,7 +204,34 @@ ViewBatch single_view_batch(int w, int h, int ts, uint32_t tile_w, uint32_t tile
   b.v[0].h = h;
   b.v[0].tile_w = int(tile_w);
   b.v[0].tile_h = int(tile_h);
+  fill_sb_layout(&b);
   return b;
+}
+
+TileWs carve_tiles(void* ws, uint32_t n, uint32_t tile_w, uint32_t tile_h, uint64_t pairs) {
+  const uint32_t npad = ceil_div(n > 0 ? n : 1, kSortTile) * kSortTile;
+  const size_t cap = pairs > 0 ? pairs : 1;
+  const ViewBatch b = single_view_batch(int(tile_w) * 8, int(tile_h) * 8, 8, tile_w, tile_h);
+  Carver c(ws);
+  TileWs t;
+  t.flags = c.take<uint32_t>(16);
+  t.rect = c.take<uint2>(n + 1);
+  t.cnt = c.take<uint32_t>(size_t(n) + 1);
+  t.dka = c.take<uint32_t>(npad);
+  t.dva = c.take<uint32_t>(npad);
+  t.dkb = c.take<uint32_t>(npad);
+  t.dvb = c.take<uint32_t>(npad);
+  const size_t hw = radix_hist_words(npad);
+  t.hist = c.take<uint32_t>(hw);
+  size_t sw = lists_scan_words(b, npad);
+  if (hw > sw) sw = hw;
+  if (size_t(n) + 1 > sw) sw = size_t(n) + 1;
+  t.scan_tmp = c.take<uint32_t>(scan_tmp_words(sw));
+  size_t dummy;
+  carve_lists(c, b, npad, cap, &t.lists, &dummy);
+  t.out_tile = c.take<uint32_t>(cap);
+  t.bytes = c.off;
+  return t;
 }
 
 // counts only: prep + sum
@@ -179,11 +245,12 @@ int tiles_count(cudaStream_t st, uint32_t n, const float* xyd, const float* aabb
   *num_pairs = 0;
   if (n == 0 || tile_w == 0 || tile_h == 0) return DSPLAT_OK;
   k_prep_tiles<<<blocks_for(n, 256), 256, 0, st>>>(n, xyd, aabb, rad, int(ts), int(tile_w), int(tile_h), t.rect,
-                                                  t.dka, t.cnt); count_launch();
+                                                  t.dka, t.cnt);
+  count_launch();
   TRY_CUDA(cudaMemsetAsync(t.cnt + n, 0, sizeof(uint32_t), st), "memset");
-  TRY_CUDA(exclusive_scan(st, t.cnt, t.off, size_t(n) + 1, t.scan_tmp), "scan");
+  TRY_CUDA(exclusive_scan(st, t.cnt, t.dkb, size_t(n) + 1, t.scan_tmp), "scan");
   uint32_t total = 0;
-  TRY_CUDA(cudaMemcpyAsync(&total, t.off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "memcpy");
+  TRY_CUDA(cudaMemcpyAsync(&total, t.dkb + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "memcpy");
   TRY_CUDA(cudaStreamSynchronize(st), "sync");
   *num_pairs = total;
   return DSPLAT_OK;
@@ -193,6 +260,8 @@ int tiles_fill(cudaStream_t st, uint32_t n, const float* xyd, const float* aabb,
                int img_h, uint32_t tile_w, uint32_t tile_h, uint32_t ts, uint32_t* tile2idx, uint32_t* idx2pnt,
                uint64_t capacity, uint64_t* keys64, void* ws, size_t ws_bytes) {
   if (!ts_ok(ts)) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
+  if ((tile_w + 7) / 8 > 255 || (tile_h + 7) / 8 > 255)
+    return fail(DSPLAT_ERR_UNSUPPORTED, "image too large for the tile size (at most 255x255 superblocks)");
   if (!tile2idx || (!idx2pnt && capacity > 0)) return fail(DSPLAT_ERR_INVALID_ARG, "null output");
   if (n > 0 && !xyd) return fail(DSPLAT_ERR_INVALID_ARG, "null input");
   TileWs t = carve_tiles(nullptr, n, tile_w, tile_h, capacity);
@@ -200,37 +269,26 @@ int tiles_fill(cudaStream_t st, uint32_t n, const float* xyd, const float* aabb,
   t = carve_tiles(ws, n, tile_w, tile_h, capacity);
   const uint32_t T = tile_w * tile_h;
   TRY_CUDA(cudaMemsetAsync(t.flags, 0, 16 * sizeof(uint32_t), st), "memset");
-  if (n == 0 || T == 0) {
+  if (n == 0 || T == 0 || capacity == 0) {
     TRY_CUDA(cudaMemsetAsync(tile2idx, 0, (size_t(T) + 1) * sizeof(uint32_t), st), "memset");
     return DSPLAT_OK;
   }
   const uint32_t npad = ceil_div(n, kSortTile) * kSortTile;
   ViewBatch b = single_view_batch(img_w, img_h, int(ts), tile_w, tile_h);
-  k_iota_pad<<<blocks_for(npad, 256), 256, 0, st>>>(t.dva, t.dka, n, npad, 1); count_launch();
+  k_iota_pad<<<blocks_for(npad, 256), 256, 0, st>>>(t.dva, t.dka, n, npad, 1);
+  count_launch();
   k_prep_tiles<<<blocks_for(n, 256), 256, 0, st>>>(n, xyd, aabb, rad, int(ts), int(tile_w), int(tile_h), t.rect,
-                                                  t.dka, t.cnt); count_launch();
+                                                  t.dka, t.cnt);
+  count_launch();
   bool in_b = false;
   TRY_CUDA(radix_sort(st, t.dka, t.dva, t.dkb, t.dvb, npad, nullptr, 32, 1, t.hist, t.scan_tmp, &in_b), "depth sort");
   const uint32_t* order = in_b ? t.dvb : t.dva;
-  k_gather_counts<<<blocks_for(size_t(npad) + 1, 256), 256, 0, st>>>(order, t.cnt, n, npad, 1, t.cs); count_launch();
-  TRY_CUDA(exclusive_scan(st, t.cs, t.off, size_t(npad) + 1, t.scan_tmp), "scan");
-  k_copy_total<<<1, 32, 0, st>>>(t.off, npad, t.flags + 1); count_launch();
-  if (capacity > 0) {
-    // the caller's idx2pnt is the second value buffer of the tile sort
-    k_emit_pairs<<<blocks_for(npad, 256), 256, 0, st>>>(order, t.cs, t.off, t.rect, n, npad, 1, b, capacity, t.pka,
-                                                        t.pva, t.flags); count_launch();
-    const int bits = bits_for(T);
-    TRY_CUDA(radix_sort(st, t.pka, t.pva, t.pkb, idx2pnt, capacity, t.flags + 1, bits, 1, t.hist, t.scan_tmp, &in_b),
-             "tile sort");
-    const uint32_t* skeys = in_b ? t.pkb : t.pka;
-    if (!in_b) k_copy_u32_count<<<1024, 256, 0, st>>>(t.pva, idx2pnt, t.flags + 1, capacity); count_launch();
-    k_item_ranges<<<1184, 256, 0, st>>>(skeys, t.flags + 1, capacity, T, tile2idx); count_launch();
-    if (keys64)
-      k_make_keys64<<<1184, 256, 0, st>>>(skeys, idx2pnt, xyd, t.flags + 1, capacity, keys64); count_launch();
-  } else {
-    uint32_t* fake = t.pka;
-    TRY_CUDA(cudaMemsetAsync(fake, 0, sizeof(uint32_t), st), "memset");
-    k_item_ranges<<<1, 32, 0, st>>>(fake, fake, 0, T, tile2idx); count_launch();
+  int rc = build_lists(st, b, n, npad, order, t.rect, t.lists, t.scan_tmp, tile2idx, idx2pnt,
+                       keys64 ? t.out_tile : nullptr, capacity, t.flags);
+  if (rc) return rc;
+  if (keys64) {
+    k_make_keys64<<<1184, 256, 0, st>>>(t.out_tile, idx2pnt, xyd, t.flags + 1, capacity, keys64);
+    count_launch();
   }
   TRY_CUDA(cudaGetLastError(), "launch");
   return DSPLAT_OK;
@@ -244,13 +302,13 @@ struct BatchWs {
   uint32_t* flags;
   float4* rec;
   uint2* rect;
-  uint32_t *cnt, *dka, *dva, *dkb, *dvb, *cs, *off, *hist, *scan_tmp, *pka, *pva, *pkb, *pvb, *item_start;
+  uint32_t *cnt, *dka, *dva, *dkb, *dvb, *hist, *scan_tmp, *item_start, *idx2pnt;
+  ListsWs lists;
   float* pix_T;
   uint32_t* pix_stop;
   float* grad_pix;
-  float* item_loss;
+  float* slab_loss;
   float4* grad2d;
-  bool order_in_b, pairs_in_b;
 };
 
 int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, ViewBatch* b) {
@@ -264,8 +322,8 @@ int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, Vi
   uint64_t items = 0, pix = 0;
   for (int v = 0; v < nv; ++v) {
     const dsplat_view& s = views[v];
-    if (s.width <= 0 || s.height <= 0 || s.width > 65535 * 8 || s.height > 65535 * 8)
-      return fail(DSPLAT_ERR_INVALID_ARG, "bad view size");
+    if (s.width <= 0 || s.height <= 0 || s.width > 16384 || s.height > 16384)
+      return fail(DSPLAT_ERR_INVALID_ARG, "bad view size (1..16384 pixels per side)");
     ViewDev& d = b->v[v];
     memcpy(d.mvp, s.mvp, sizeof(d.mvp));
     memcpy(d.campos, s.campos, sizeof(d.campos));
@@ -273,6 +331,8 @@ int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, Vi
     d.h = s.height;
     d.tile_w = (s.width + ts - 1) / ts;
     d.tile_h = (s.height + ts - 1) / ts;
+    if ((d.tile_w + 7) / 8 > 255 || (d.tile_h + 7) / 8 > 255)
+      return fail(DSPLAT_ERR_UNSUPPORTED, "view too large for the tile size (at most 255x255 superblocks)");
     d.item_base = uint32_t(items);
     d.pix_base = uint32_t(pix);
     items += uint64_t(d.tile_w) * d.tile_h;
@@ -281,6 +341,7 @@ int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, Vi
   if (items >= 0xffffffffull || pix * 3 >= 0xffffffffull) return fail(DSPLAT_ERR_INVALID_ARG, "batch too large");
   b->num_items = uint32_t(items);
   b->num_pix = uint32_t(pix);
+  fill_sb_layout(b);
   return DSPLAT_OK;
 }
 
@@ -296,37 +357,27 @@ BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity)
   L.num_items = b.num_items;
   L.num_pix = b.num_pix;
   L.npad = npad;
-  L.tile_sort_bits = uint32_t(bits_for(b.num_items));
+  L.slabs_per_tile = b.ts == 32 ? 4u : 1u;
   w.flags = c.take<uint32_t>(16, &L.off_flags);
   w.rec = c.take<float4>(3 * VN + 3, &L.off_rec);
   w.rect = c.take<uint2>(VN + 1, &L.off_rect);
   w.cnt = c.take<uint32_t>(VN + 1, &L.off_cnt);
-  size_t off_a, off_b;
   w.dka = c.take<uint32_t>(Vp);
-  w.dva = c.take<uint32_t>(Vp, &off_a);
+  w.dva = c.take<uint32_t>(Vp, &L.off_order);  // 4 passes of 8 bits end back in (dka, dva)
   w.dkb = c.take<uint32_t>(Vp);
-  w.dvb = c.take<uint32_t>(Vp, &off_b);
-  w.order_in_b = false;  // 4 passes of 8 bits end in the first buffer pair
-  L.off_order = off_a;
-  w.cs = c.take<uint32_t>(Vp + 1);
-  w.off = c.take<uint32_t>(Vp + 1);
-  const size_t hw = radix_hist_words(Vp > cap ? Vp : cap);
+  w.dvb = c.take<uint32_t>(Vp);
+  const size_t hw = radix_hist_words(Vp);
   w.hist = c.take<uint32_t>(hw);
-  w.scan_tmp = c.take<uint32_t>(scan_tmp_words(hw > Vp + 1 ? hw : Vp + 1));
-  size_t ok_a, ov_a, ok_b, ov_b;
-  w.pka = c.take<uint32_t>(cap, &ok_a);
-  w.pva = c.take<uint32_t>(cap, &ov_a);
-  w.pkb = c.take<uint32_t>(cap, &ok_b);
-  w.pvb = c.take<uint32_t>(cap, &ov_b);
-  const int passes = (int(L.tile_sort_bits) + 7) / 8;
-  w.pairs_in_b = (passes % 2) == 1;
-  L.off_idx2pnt = w.pairs_in_b ? ov_b : ov_a;
-  L.off_item_key = w.pairs_in_b ? ok_b : ok_a;
+  size_t sw = lists_scan_words(b, npad);
+  if (hw > sw) sw = hw;
+  w.scan_tmp = c.take<uint32_t>(scan_tmp_words(sw));
+  carve_lists(c, b, npad, cap, &w.lists, &L.off_sb_list);
   w.item_start = c.take<uint32_t>(size_t(b.num_items) + 1, &L.off_item_start);
+  w.idx2pnt = c.take<uint32_t>(cap, &L.off_idx2pnt);
   w.pix_T = c.take<float>(b.num_pix, &L.off_pix_T);
   w.pix_stop = c.take<uint32_t>(b.num_pix, &L.off_pix_stop);
   w.grad_pix = c.take<float>(size_t(b.num_pix) * 3, &L.off_grad_pix);
-  w.item_loss = c.take<float>(b.num_items, &L.off_item_loss);
+  w.slab_loss = c.take<float>(size_t(b.num_items) * L.slabs_per_tile, &L.off_slab_loss);
   w.grad2d = c.take<float4>(3 * VN + 3, &L.off_grad2d);
   L.total_bytes = align_up(c.off, 256);
   return w;
@@ -526,35 +577,31 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
   if (n == 0 || pair_capacity == 0) {
     TRY_CUDA(cudaMemsetAsync(w.item_start, 0, (size_t(b.num_items) + 1) * 4, st), "memset");
   } else {
-    k_iota_pad<<<blocks_for(Vp, 256), 256, 0, st>>>(w.dva, w.dka, n, npad, V); count_launch();
+    k_iota_pad<<<blocks_for(Vp, 256), 256, 0, st>>>(w.dva, w.dka, n, npad, V);
+    count_launch();
     k_fused_project<<<blocks_for(n, 128), 128, 0, st>>>(n, npad, params->sh_degree, params->means,
                                                         params->log_scales, params->quats, params->opacity,
-                                                        params->colors, b, w.rec, w.rect, w.dka, w.cnt); count_launch();
+                                                        params->colors, b, w.rec, w.rect, w.dka, w.cnt);
+    count_launch();
     stage_mark(st, 1);
     bool in_b = false;
     TRY_CUDA(radix_sort(st, w.dka, w.dva, w.dkb, w.dvb, Vp, nullptr, 32, V, w.hist, w.scan_tmp, &in_b), "depth sort");
     stage_mark(st, 2);
     const uint32_t* order = in_b ? w.dvb : w.dva;
-    k_gather_counts<<<blocks_for(Vp + 1, 256), 256, 0, st>>>(order, w.cnt, n, npad, V, w.cs); count_launch();
-    TRY_CUDA(exclusive_scan(st, w.cs, w.off, Vp + 1, w.scan_tmp), "scan");
-    k_copy_total<<<1, 32, 0, st>>>(w.off, Vp, w.flags + 1); count_launch();
-    k_emit_pairs<<<blocks_for(Vp, 256), 256, 0, st>>>(order, w.cs, w.off, w.rect, n, npad, V, b, pair_capacity, w.pka,
-                                                      w.pva, w.flags); count_launch();
+    int rc2 = build_lists(st, b, n, npad, order, w.rect, w.lists, w.scan_tmp, w.item_start, w.idx2pnt, nullptr,
+                          pair_capacity, w.flags);
+    if (rc2) return rc2;
     stage_mark(st, 3);
-    TRY_CUDA(radix_sort(st, w.pka, w.pva, w.pkb, w.pvb, pair_capacity, w.flags + 1, int(w.L.tile_sort_bits), 1,
-                        w.hist, w.scan_tmp, &in_b),
-             "tile sort");
-    const uint32_t* skeys = in_b ? w.pkb : w.pka;
-    k_item_ranges<<<1184, 256, 0, st>>>(skeys, w.flags + 1, pair_capacity,
-                                                                      b.num_items, w.item_start); count_launch();
   }
   stage_mark(st, 4);
-  const uint32_t* idx2pnt = w.pairs_in_b ? w.pvb : w.pva;
-  TRY_CUDA(raster_fwd(st, b, n, w.rec, w.item_start, idx2pnt, w.flags + 2, out_rgb, w.pix_T, w.pix_stop, target,
-                      w.grad_pix, w.item_loss),
+  TRY_CUDA(raster_fwd(st, b, n, w.rec, w.item_start, w.idx2pnt, w.flags + 2, out_rgb, w.pix_T, w.pix_stop, target,
+                      w.grad_pix, w.slab_loss),
            "raster_fwd");
   stage_mark(st, 5);
-  if (out_alpha) k_one_minus<<<blocks_for(b.num_pix, 256), 256, 0, st>>>(w.pix_T, out_alpha, b.num_pix); count_launch();
+  if (out_alpha) {
+    k_one_minus<<<blocks_for(b.num_pix, 256), 256, 0, st>>>(w.pix_T, out_alpha, b.num_pix);
+    count_launch();
+  }
   TRY_CUDA(cudaGetLastError(), "forward");
   return DSPLAT_OK;
 }
@@ -581,8 +628,7 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
   TRY_CUDA(cudaMemsetAsync(w.grad2d, 0, 3 * VN * sizeof(float4), st), "memset");
   TRY_CUDA(cudaMemsetAsync(w.flags + 3, 0, sizeof(uint32_t), st), "memset");
   stage_mark(st, 7);
-  const uint32_t* idx2pnt = w.pairs_in_b ? w.pvb : w.pva;
-  TRY_CUDA(raster_bwd(st, b, n, w.rec, w.item_start, idx2pnt, w.flags + 3, grad_rgb ? grad_rgb : w.grad_pix, w.pix_T,
+  TRY_CUDA(raster_bwd(st, b, n, w.rec, w.item_start, w.idx2pnt, w.flags + 3, grad_rgb ? grad_rgb : w.grad_pix, w.pix_T,
                       w.pix_stop, w.grad2d),
            "raster_bwd");
   stage_mark(st, 8);

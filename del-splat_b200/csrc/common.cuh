@@ -8,7 +8,6 @@
 #include <atomic>
 
 #define DSPLAT_MAX_VIEWS 32
-#define DSPLAT_SB_TILES 8  // unused by the LSD pipeline; kept for layout docs
 
 namespace dsplat {
 
@@ -26,7 +25,7 @@ struct ViewDev {
   int32_t tile_w, tile_h;
   uint32_t item_base;  // first global (view, tile) item of this view
   uint32_t pix_base;   // first pixel of this view in the concatenated images
-  int32_t pad;
+  uint32_t sb_base;    // first superblock (8x8 tiles) of this view
 };
 
 struct ViewBatch {
@@ -34,6 +33,8 @@ struct ViewBatch {
   int32_t ts;          // tile size in pixels (8, 16 or 32)
   uint32_t num_items;  // sum of tile counts
   uint32_t num_pix;    // sum of pixel counts
+  uint32_t num_sb;     // sum of superblock counts
+  uint32_t max_sb;     // largest per-view superblock count
   ViewDev v[DSPLAT_MAX_VIEWS];
 };
 

@@ -6,260 +6,230 @@
 // e = exp(-q/2) * opacity with q = d^T conic d; rgb += c*T*e; T *= 1-e;
 // alpha_sum += T*e; stop once alpha_sum > 0.999.
 //
-// B200 structure: one CTA per (view, tile) work item, TS*TS threads = one
-// pixel each.  Entries are staged cooperatively into shared memory in batches
-// of TS*TS (one coalesced index load + one 48-byte record gather per thread),
-// every pixel then walks the batch from shared memory.  A CTA stops loading
-// as soon as __syncthreads_count says every pixel has terminated.  The
-// fused-path kernels are persistent: CTAs pull items from a global counter
-// (work stealing), so views of different resolutions share one launch.
+// B200 structure: the unit of work is a warp task = one slab of 256 pixels
+// of one (view, tile) item (a 16x16 tile, a 32x8 quarter of a 32x32 tile or
+// a whole 8x8 tile); each lane owns 8 pixels of one column (2 for 8x8 tiles).
+// A warp stages 32 list entries at a time into its own shared-memory slots
+// (one coalesced index load + one 48-byte record gather per lane), then every
+// lane walks them with 128-bit broadcast reads, amortising each read over its
+// pixels.  The warp stops fetching as soon as all its pixels terminated
+// (__any_sync), so no CTA-wide barrier exists anywhere.  Warps pull tasks
+// from a global counter (work stealing): one persistent launch covers views
+// of different resolutions.
 //
-// The blend arithmetic uses non-contracted IEEE operations and dexp() so that
-// the oracle reproduces it exactly, including every early-exit decision.
+// The blend arithmetic uses non-contracted IEEE operations and dexp() so the
+// oracle reproduces it exactly, including every early-exit decision.
 //
 // Backward (no reference counterpart): the same walk in reverse
 // (back-to-front) from the saved stop position up to the list end; the
 // transmittance in front of each entry is rebuilt from the saved final value,
 // T_i = T_{i+1} / (1 - e_i), and the colour behind it is accumulated, so no
-// per-pixel list is stored.  Per-entry gradients are summed across the warp
-// with shuffles and added to the per-(view, point) 2D gradient with one
-// vectorised float4 atomic per component group.
+// per-pixel list is stored.  Each lane sums its pixels' contributions in
+// registers, the warp sums them with shuffles (once per entry for 256
+// pixels) and one lane adds them to the per-(view, point) 2D gradient with
+// vectorised float4 atomics.
 #include "common.cuh"
 
 namespace dsplat {
 
-struct SmemEnt {
-  float* px;
-  float* py;
-  float* a;
-  float* b;
-  float* c;
-  float* op;
-  float* r;
-  float* g;
-  float* bl;
-  float* x0;
-  float* y0;
-  float* x1;
-  float* y1;
-  uint32_t* gid;
+constexpr int kRasterWarps = 4;  // warps per CTA (independent tasks)
+
+struct Ent {  // one staged list entry (64 bytes)
+  float4 a;   // px, py, conic A, conic B
+  float4 b;   // conic C, opacity, r, g
+  float4 c;   // b, box x0, box y0, box x1
+  float4 d;   // box y1, point index (bits), -, -
 };
 
-template <int NT>
-__device__ __forceinline__ SmemEnt carve(float* s) {
-  SmemEnt e;
-  e.px = s;
-  e.py = s + NT;
-  e.a = s + 2 * NT;
-  e.b = s + 3 * NT;
-  e.c = s + 4 * NT;
-  e.op = s + 5 * NT;
-  e.r = s + 6 * NT;
-  e.g = s + 7 * NT;
-  e.bl = s + 8 * NT;
-  e.x0 = s + 9 * NT;
-  e.y0 = s + 10 * NT;
-  e.x1 = s + 11 * NT;
-  e.y1 = s + 12 * NT;
-  e.gid = reinterpret_cast<uint32_t*>(s + 13 * NT);
-  return e;
-}
-constexpr int kSmemFloatsPerEnt = 14;
+template <int TS>
+struct Geo {
+  static constexpr int PPL = TS == 8 ? 2 : 8;   // pixels per lane
+  static constexpr int ROW_STEP = 32 / TS;        // rows covered by the 32 lanes at once
+  static constexpr int SLAB_ROWS = ROW_STEP * PPL;
+  static constexpr int SLABS = TS / SLAB_ROWS;    // warp tasks per tile
+  static_assert(SLABS * SLAB_ROWS == TS, "slab geometry");
+};
 
-__device__ __forceinline__ void stage_packed(const SmemEnt& S, int j, const float4* __restrict__ rec, uint32_t g) {
+__device__ __forceinline__ void stage_packed(Ent* dst, const float4* __restrict__ rec, uint32_t g) {
   const float4 r0 = __ldg(rec + 3 * size_t(g));
   const float4 r1 = __ldg(rec + 3 * size_t(g) + 1);
   const float4 r2 = __ldg(rec + 3 * size_t(g) + 2);
-  S.px[j] = r0.x;
-  S.py[j] = r0.y;
-  S.a[j] = r0.z;
-  S.b[j] = r0.w;
-  S.c[j] = r1.x;
-  S.op[j] = r1.y;
-  S.r[j] = r1.z;
-  S.g[j] = r1.w;
-  S.bl[j] = r2.x;
-  S.x0[j] = fs(r0.x, r2.y);
-  S.y0[j] = fs(r0.y, r2.z);
-  S.x1[j] = fa(r0.x, r2.y);
-  S.y1[j] = fa(r0.y, r2.z);
-  S.gid[j] = g;
+  dst->a = r0;
+  dst->b = r1;
+  dst->c = make_float4(r2.x, fs(r0.x, r2.y), fs(r0.y, r2.z), fa(r0.x, r2.y));
+  dst->d = make_float4(fa(r0.y, r2.z), __uint_as_float(g), 0.f, 0.f);
 }
 
-__device__ __forceinline__ void stage_aos(const SmemEnt& S, int j, const float* __restrict__ xyd,
-                                          const float* __restrict__ conic, const float* __restrict__ aabb,
-                                          const float* __restrict__ opacity, const float* __restrict__ rgb,
-                                          uint32_t g) {
-  S.px[j] = xyd[3 * size_t(g)];
-  S.py[j] = xyd[3 * size_t(g) + 1];
-  S.a[j] = conic[3 * size_t(g)];
-  S.b[j] = conic[3 * size_t(g) + 1];
-  S.c[j] = conic[3 * size_t(g) + 2];
-  S.op[j] = opacity[g];
-  S.r[j] = rgb[3 * size_t(g)];
-  S.g[j] = rgb[3 * size_t(g) + 1];
-  S.bl[j] = rgb[3 * size_t(g) + 2];
-  S.x0[j] = aabb[4 * size_t(g)];
-  S.y0[j] = aabb[4 * size_t(g) + 1];
-  S.x1[j] = aabb[4 * size_t(g) + 2];
-  S.y1[j] = aabb[4 * size_t(g) + 3];
-  S.gid[j] = g;
-}
-
-struct PixState {
-  float T, asum, c0, c1, c2;
-  uint32_t last;
-  bool done;
+struct AosSrc {
+  const float *xyd, *conic, *aabb, *opacity, *rgb;
+  __device__ __forceinline__ void stage(Ent* dst, uint32_t g) const {
+    const size_t i = g;
+    dst->a = make_float4(xyd[3 * i], xyd[3 * i + 1], conic[3 * i], conic[3 * i + 1]);
+    dst->b = make_float4(conic[3 * i + 2], opacity[i], rgb[3 * i], rgb[3 * i + 1]);
+    dst->c = make_float4(rgb[3 * i + 2], aabb[4 * i], aabb[4 * i + 1], aabb[4 * i + 2]);
+    dst->d = make_float4(aabb[4 * i + 3], __uint_as_float(g), 0.f, 0.f);
+  }
 };
 
-// Walks staged entries j = 0..cnt-1 (entry j sits at list position hi-1-j).
-__device__ __forceinline__ void blend_batch(const SmemEnt& S, int cnt, uint32_t hi, float fx, float fy,
-                                            PixState& st) {
-  if (st.done) return;
-  for (int j = 0; j < cnt; ++j) {
-    if (!(S.x0[j] <= fx && fx <= S.x1[j] && S.y0[j] <= fy && fy <= S.y1[j])) continue;
-    const float dx = fs(fx, S.px[j]);
-    const float dy = fs(fy, S.py[j]);
-    const float q = fa(fa(fm(fm(S.a[j], dx), dx), fm(S.b[j], fa(fm(dx, dy), fm(dy, dx)))), fm(fm(S.c[j], dy), dy));
-    const float e = fm(dexp(fm(-0.5f, q)), S.op[j]);
-    const float eo = fm(st.T, e);
-    st.c0 = fa(st.c0, fm(S.r[j], eo));
-    st.c1 = fa(st.c1, fm(S.g[j], eo));
-    st.c2 = fa(st.c2, fm(S.bl[j], eo));
-    st.T = fm(st.T, fs(1.f, e));
-    st.asum = fa(st.asum, eo);
-    if (st.asum >= kAlphaBreak) {
-      st.done = true;
-      st.last = hi - 1u - uint32_t(j);
-      return;
+struct PackedSrc {
+  const float4* rec;
+  __device__ __forceinline__ void stage(Ent* dst, uint32_t g) const { stage_packed(dst, rec, g); }
+};
+
+// q = d^T K d exactly as the reference's mult_vec_from_both_sides orders it:
+// (A dx) dx + B (dx dy + dy dx) + (C dy) dy
+__device__ __forceinline__ float quad(float B, float C, float dx, float dy, float adxdx) {
+  const float t = fm(dx, dy);
+  return fa(fa(adxdx, fm(B, fa(t, fm(dy, dx)))), fm(fm(C, dy), dy));
+}
+
+// ---------------------------------------------------------------------------
+// Forward walk of one slab by one warp.
+// ---------------------------------------------------------------------------
+template <int TS, class Src>
+__device__ __forceinline__ void fwd_slab(const Src& src, Ent* sm, const uint32_t* __restrict__ idx2pnt, uint32_t s,
+                                         uint32_t e, int px0, int py0, int w, int h, bool accumulate,
+                                         float* __restrict__ out_rgb, size_t pix_base, float* __restrict__ out_T,
+                                         uint32_t* __restrict__ out_last, const float* __restrict__ target,
+                                         float* __restrict__ grad_pix, float* __restrict__ loss_slot) {
+  using G = Geo<TS>;
+  constexpr int PPL = G::PPL;
+  const int lane = threadIdx.x & 31;
+  const int ix = px0 + (lane % TS);
+  const int iy0 = py0 + (lane / TS);
+  const float fx = float(ix) + 0.5f;
+  float T[PPL], as[PPL], c0[PPL], c1[PPL], c2[PPL];
+  uint32_t last[PPL];
+  uint32_t live = 0;
+#pragma unroll
+  for (int k = 0; k < PPL; ++k) {
+    const int iy = iy0 + k * G::ROW_STEP;
+    T[k] = 1.f;
+    as[k] = 0.f;
+    c0[k] = c1[k] = c2[k] = 0.f;
+    last[k] = s;
+    if (ix < w && iy < h) {
+      live |= 1u << k;
+      if (accumulate) {
+        const size_t p = pix_base + size_t(iy) * w + ix;
+        c0[k] = out_rgb[3 * p];
+        c1[k] = out_rgb[3 * p + 1];
+        c2[k] = out_rgb[3 * p + 2];
+      }
     }
+  }
+  const uint32_t inside = live;
+  for (uint32_t hi = e; hi > s;) {
+    const int cnt = int(min(32u, hi - s));
+    if (lane < cnt) src.stage(&sm[lane], idx2pnt[hi - 1u - uint32_t(lane)]);
+    __syncwarp();
+    if (live) {
+      for (int j = 0; j < cnt; ++j) {
+        const float4 ea = sm[j].a, eb = sm[j].b, ec = sm[j].c, ed = sm[j].d;
+        if (!(ec.y <= fx && fx <= ec.w)) continue;
+        const float dx = fs(fx, ea.x);
+        const float adxdx = fm(fm(ea.z, dx), dx);
+#pragma unroll
+        for (int k = 0; k < PPL; ++k) {
+          if (!((live >> k) & 1u)) continue;
+          const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
+          if (!(ec.z <= fy && fy <= ed.x)) continue;
+          const float dy = fs(fy, ea.y);
+          const float q = quad(ea.w, eb.x, dx, dy, adxdx);
+          const float al = fm(dexp(fm(-0.5f, q)), eb.y);
+          const float eo = fm(T[k], al);
+          c0[k] = fa(c0[k], fm(eb.z, eo));
+          c1[k] = fa(c1[k], fm(eb.w, eo));
+          c2[k] = fa(c2[k], fm(ec.x, eo));
+          T[k] = fm(T[k], fs(1.f, al));
+          as[k] = fa(as[k], eo);
+          if (as[k] >= kAlphaBreak) {
+            live &= ~(1u << k);
+            last[k] = hi - 1u - uint32_t(j);
+          }
+        }
+        if (!live) break;
+      }
+    }
+    hi -= uint32_t(cnt);
+    if (!__any_sync(0xffffffffu, live != 0u)) break;
+    __syncwarp();
+  }
+  float l = 0.f;
+#pragma unroll
+  for (int k = 0; k < PPL; ++k) {
+    if (!((inside >> k) & 1u)) continue;
+    const int iy = iy0 + k * G::ROW_STEP;
+    const size_t p = pix_base + size_t(iy) * w + ix;
+    out_rgb[3 * p] = c0[k];
+    out_rgb[3 * p + 1] = c1[k];
+    out_rgb[3 * p + 2] = c2[k];
+    if (out_T) out_T[p] = T[k];
+    if (out_last) out_last[p] = last[k];
+    if (target) {
+      const float d0 = c0[k] - target[3 * p], d1 = c1[k] - target[3 * p + 1], d2 = c2[k] - target[3 * p + 2];
+      grad_pix[3 * p] = 2.f * d0;
+      grad_pix[3 * p + 1] = 2.f * d1;
+      grad_pix[3 * p + 2] = 2.f * d2;
+      l += d0 * d0 + d1 * d1 + d2 * d2;
+    }
+  }
+  if (target) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if (lane == 0) *loss_slot = l;
   }
 }
 
 // ---------------------------------------------------------------------------
-// Fused-path forward: persistent, work-stealing over (view, tile) items.
-// outputs (per pixel of the concatenated images): rgb[3], T, last list pos.
-// If `target` is given, also writes the L2-loss pixel gradient 2(C - target)
-// and per-item partial losses.
+// Fused-path forward: persistent, per-warp work stealing over slab tasks.
+// slab_loss: one partial L2 loss per task (when target is given).
 // ---------------------------------------------------------------------------
 template <int TS>
-__global__ void __launch_bounds__(TS* TS) k_raster_fwd(const ViewBatch b, uint32_t n, const float4* __restrict__ rec,
-                                                      const uint32_t* __restrict__ item_start,
-                                                      const uint32_t* __restrict__ idx2pnt,
-                                                      uint32_t* __restrict__ work_counter, float* __restrict__ out_rgb,
-                                                      float* __restrict__ out_T, uint32_t* __restrict__ out_last,
-                                                      const float* __restrict__ target, float* __restrict__ grad_pix,
-                                                      float* __restrict__ item_loss) {
-  constexpr int NT = TS * TS;
-  extern __shared__ float smem[];
-  const SmemEnt S = carve<NT>(smem);
-  __shared__ uint32_t s_item;
-  __shared__ float s_loss[NT / 32];
-  const int tid = threadIdx.x;
+__global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
+    const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint32_t* __restrict__ item_start,
+    const uint32_t* __restrict__ idx2pnt, uint32_t* __restrict__ work_counter, float* __restrict__ out_rgb,
+    float* __restrict__ out_T, uint32_t* __restrict__ out_last, const float* __restrict__ target,
+    float* __restrict__ grad_pix, float* __restrict__ slab_loss) {
+  using G = Geo<TS>;
+  __shared__ Ent sm_all[kRasterWarps][32];
+  Ent* sm = sm_all[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const uint32_t num_tasks = b.num_items * G::SLABS;
   for (;;) {
-    if (tid == 0) s_item = atomicAdd(work_counter, 1u);
-    __syncthreads();
-    const uint32_t item = s_item;
-    __syncthreads();
-    if (item >= b.num_items) return;
+    uint32_t task = 0;
+    if (lane == 0) task = atomicAdd(work_counter, 1u);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (task >= num_tasks) return;
+    const uint32_t item = task / G::SLABS, slab = task % G::SLABS;
     const int v = view_of_item(b, item);
     const ViewDev& vd = b.v[v];
     const uint32_t t = item - vd.item_base;
-    const int ix = int(t % uint32_t(vd.tile_w)) * TS + (tid % TS);
-    const int iy = int(t / uint32_t(vd.tile_w)) * TS + (tid / TS);
-    const bool inside = ix < vd.w && iy < vd.h;
-    const float fx = float(ix) + 0.5f, fy = float(iy) + 0.5f;
-    const uint32_t s = item_start[item], e = item_start[item + 1];
-    PixState st{1.f, 0.f, 0.f, 0.f, 0.f, s, !inside};
-    const float4* recv = rec + 3 * size_t(v) * n;
-    for (uint32_t hi = e; hi > s;) {
-      const int cnt = int(min(uint32_t(NT), hi - s));
-      if (tid < cnt) {
-        const uint32_t g = idx2pnt[hi - 1u - uint32_t(tid)];
-        stage_packed(S, tid, recv, g);
-      }
-      __syncthreads();
-      blend_batch(S, cnt, hi, fx, fy, st);
-      hi -= uint32_t(cnt);
-      if (__syncthreads_count(!st.done) == 0) break;
-    }
-    float l = 0.f;
-    if (inside) {
-      const size_t pix = size_t(vd.pix_base) + size_t(iy) * vd.w + ix;
-      out_rgb[3 * pix] = st.c0;
-      out_rgb[3 * pix + 1] = st.c1;
-      out_rgb[3 * pix + 2] = st.c2;
-      out_T[pix] = st.T;
-      out_last[pix] = st.last;
-      if (target) {
-        const float d0 = st.c0 - target[3 * pix], d1 = st.c1 - target[3 * pix + 1],
-                    d2 = st.c2 - target[3 * pix + 2];
-        grad_pix[3 * pix] = 2.f * d0;
-        grad_pix[3 * pix + 1] = 2.f * d1;
-        grad_pix[3 * pix + 2] = 2.f * d2;
-        l = d0 * d0 + d1 * d1 + d2 * d2;
-      }
-    }
-    if (target) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-      if ((tid & 31) == 0) s_loss[tid >> 5] = l;
-      __syncthreads();
-      if (tid == 0) {
-        float acc = 0.f;
-        for (int w = 0; w < NT / 32; ++w) acc += s_loss[w];
-        item_loss[item] = acc;
-      }
-    }
-    __syncthreads();
+    const int px0 = int(t % uint32_t(vd.tile_w)) * TS;
+    const int py0 = int(t / uint32_t(vd.tile_w)) * TS + int(slab) * G::SLAB_ROWS;
+    PackedSrc src{rec + 3 * size_t(v) * n};
+    fwd_slab<TS>(src, sm, idx2pnt, item_start[item], item_start[item + 1], px0, py0, vd.w, vd.h, false, out_rgb,
+                 vd.pix_base, out_T, out_last, target, grad_pix, slab_loss ? slab_loss + task : nullptr);
+    __syncwarp();
   }
 }
 
-// ---------------------------------------------------------------------------
-// Drop-in forward (splat_gauss.rs:46-94): AoS inputs, one CTA per tile, adds
-// into pix2rgb like the reference.  Optional T / stop-position outputs.
-// ---------------------------------------------------------------------------
+// Drop-in forward (splat_gauss.rs:46-94): AoS inputs, accumulates into pix2rgb.
 template <int TS>
-__global__ void __launch_bounds__(TS* TS) k_raster_fwd_aos(int w, int h, int tile_w, float* __restrict__ pix2rgb,
-                                                          const float* __restrict__ xyd, const float* __restrict__ conic,
-                                                          const float* __restrict__ aabb,
-                                                          const float* __restrict__ opacity,
-                                                          const float* __restrict__ rgb,
-                                                          const uint32_t* __restrict__ tile2idx,
-                                                          const uint32_t* __restrict__ idx2pnt,
-                                                          float* __restrict__ out_T, uint32_t* __restrict__ out_last) {
-  constexpr int NT = TS * TS;
-  extern __shared__ float smem[];
-  const SmemEnt S = carve<NT>(smem);
-  const int tid = threadIdx.x;
-  const uint32_t tile = blockIdx.y * uint32_t(tile_w) + blockIdx.x;
-  const int ix = int(blockIdx.x) * TS + (tid % TS), iy = int(blockIdx.y) * TS + (tid / TS);
-  const bool inside = ix < w && iy < h;
-  const float fx = float(ix) + 0.5f, fy = float(iy) + 0.5f;
-  const uint32_t s = tile2idx[tile], e = tile2idx[tile + 1];
-  PixState st{1.f, 0.f, 0.f, 0.f, 0.f, s, !inside};
-  if (inside) {
-    const size_t pix = size_t(iy) * w + ix;
-    st.c0 = pix2rgb[3 * pix];
-    st.c1 = pix2rgb[3 * pix + 1];
-    st.c2 = pix2rgb[3 * pix + 2];
-  }
-  for (uint32_t hi = e; hi > s;) {
-    const int cnt = int(min(uint32_t(NT), hi - s));
-    if (tid < cnt) stage_aos(S, tid, xyd, conic, aabb, opacity, rgb, idx2pnt[hi - 1u - uint32_t(tid)]);
-    __syncthreads();
-    blend_batch(S, cnt, hi, fx, fy, st);
-    hi -= uint32_t(cnt);
-    if (__syncthreads_count(!st.done) == 0) break;
-  }
-  if (inside) {
-    const size_t pix = size_t(iy) * w + ix;
-    pix2rgb[3 * pix] = st.c0;
-    pix2rgb[3 * pix + 1] = st.c1;
-    pix2rgb[3 * pix + 2] = st.c2;
-    if (out_T) out_T[pix] = st.T;
-    if (out_last) out_last[pix] = st.last;
-  }
+__global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
+    int w, int h, int tile_w, uint32_t num_tasks, float* __restrict__ pix2rgb, AosSrc src,
+    const uint32_t* __restrict__ tile2idx, const uint32_t* __restrict__ idx2pnt, float* __restrict__ out_T,
+    uint32_t* __restrict__ out_last) {
+  using G = Geo<TS>;
+  __shared__ Ent sm_all[kRasterWarps][32];
+  Ent* sm = sm_all[threadIdx.x >> 5];
+  const uint32_t task = blockIdx.x * kRasterWarps + (threadIdx.x >> 5);
+  if (task >= num_tasks) return;
+  const uint32_t tile = task / G::SLABS, slab = task % G::SLABS;
+  const int px0 = int(tile % uint32_t(tile_w)) * TS;
+  const int py0 = int(tile / uint32_t(tile_w)) * TS + int(slab) * G::SLAB_ROWS;
+  fwd_slab<TS>(src, sm, idx2pnt, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, true, pix2rgb, 0, out_T,
+               out_last, nullptr, nullptr, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -267,90 +237,97 @@ __global__ void __launch_bounds__(TS* TS) k_raster_fwd_aos(int w, int h, int til
 //   (d px, d py, d A, d B) (d C, d opacity, d r, d g) (d b, 0, 0, 0)
 // ---------------------------------------------------------------------------
 template <int TS>
-__global__ void __launch_bounds__(TS* TS) k_raster_bwd(const ViewBatch b, uint32_t n, const float4* __restrict__ rec,
-                                                      const uint32_t* __restrict__ item_start,
-                                                      const uint32_t* __restrict__ idx2pnt,
-                                                      uint32_t* __restrict__ work_counter,
-                                                      const float* __restrict__ grad_pix,
-                                                      const float* __restrict__ pix_T,
-                                                      const uint32_t* __restrict__ pix_last,
-                                                      float4* __restrict__ grad2d) {
-  constexpr int NT = TS * TS;
-  extern __shared__ float smem[];
-  const SmemEnt S = carve<NT>(smem);
-  __shared__ uint32_t s_item;
-  __shared__ uint32_t s_min_last;
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
+__global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
+    const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint32_t* __restrict__ item_start,
+    const uint32_t* __restrict__ idx2pnt, uint32_t* __restrict__ work_counter, const float* __restrict__ grad_pix,
+    const float* __restrict__ pix_T, const uint32_t* __restrict__ pix_last, float4* __restrict__ grad2d) {
+  using G = Geo<TS>;
+  constexpr int PPL = G::PPL;
+  __shared__ Ent sm_all[kRasterWarps][32];
+  Ent* sm = sm_all[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const uint32_t num_tasks = b.num_items * G::SLABS;
   for (;;) {
-    if (tid == 0) {
-      s_item = atomicAdd(work_counter, 1u);
-      s_min_last = 0xffffffffu;
-    }
-    __syncthreads();
-    const uint32_t item = s_item;
-    if (item >= b.num_items) return;
+    uint32_t task = 0;
+    if (lane == 0) task = atomicAdd(work_counter, 1u);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (task >= num_tasks) return;
+    const uint32_t item = task / G::SLABS, slab = task % G::SLABS;
     const int v = view_of_item(b, item);
     const ViewDev& vd = b.v[v];
     const uint32_t t = item - vd.item_base;
-    const int ix = int(t % uint32_t(vd.tile_w)) * TS + (tid % TS);
-    const int iy = int(t / uint32_t(vd.tile_w)) * TS + (tid / TS);
-    const bool inside = ix < vd.w && iy < vd.h;
-    const float fx = float(ix) + 0.5f, fy = float(iy) + 0.5f;
+    const int ix = int(t % uint32_t(vd.tile_w)) * TS + (lane % TS);
+    const int iy0 = int(t / uint32_t(vd.tile_w)) * TS + int(slab) * G::SLAB_ROWS + (lane / TS);
+    const float fx = float(ix) + 0.5f;
     const uint32_t s = item_start[item], e = item_start[item + 1];
-    float Tcur = 1.f, dC0 = 0.f, dC1 = 0.f, dC2 = 0.f;
-    uint32_t last = e;
-    if (inside) {
-      const size_t pix = size_t(vd.pix_base) + size_t(iy) * vd.w + ix;
-      Tcur = pix_T[pix];
-      last = pix_last[pix];
-      dC0 = grad_pix[3 * pix];
-      dC1 = grad_pix[3 * pix + 1];
-      dC2 = grad_pix[3 * pix + 2];
-      atomicMin(&s_min_last, last);
+    float Tc[PPL], a0[PPL], a1[PPL], a2[PPL], d0[PPL], d1[PPL], d2[PPL];
+    uint32_t last[PPL];
+    uint32_t lo_min = e;
+#pragma unroll
+    for (int k = 0; k < PPL; ++k) {
+      const int iy = iy0 + k * G::ROW_STEP;
+      a0[k] = a1[k] = a2[k] = 0.f;
+      Tc[k] = 1.f;
+      d0[k] = d1[k] = d2[k] = 0.f;
+      last[k] = e;  // outside pixels process nothing
+      if (ix < vd.w && iy < vd.h) {
+        const size_t p = size_t(vd.pix_base) + size_t(iy) * vd.w + ix;
+        Tc[k] = pix_T[p];
+        last[k] = pix_last[p];
+        d0[k] = grad_pix[3 * p];
+        d1[k] = grad_pix[3 * p + 1];
+        d2[k] = grad_pix[3 * p + 2];
+        lo_min = min(lo_min, last[k]);
+      }
     }
-    __syncthreads();
-    const uint32_t lo0 = max(s, s_min_last);
-    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lo_min = min(lo_min, __shfl_xor_sync(0xffffffffu, lo_min, o));
     const float4* recv = rec + 3 * size_t(v) * n;
     float4* gv = grad2d + 3 * size_t(v) * n;
-    for (uint32_t lo = lo0; lo < e; lo += NT) {
-      const int cnt = int(min(uint32_t(NT), e - lo));
-      if (tid < cnt) stage_packed(S, tid, recv, idx2pnt[lo + uint32_t(tid)]);
-      __syncthreads();
+    for (uint32_t lo = max(s, lo_min); lo < e; lo += 32) {
+      const int cnt = int(min(32u, e - lo));
+      if (lane < cnt) stage_packed(&sm[lane], recv, idx2pnt[lo + uint32_t(lane)]);
+      __syncwarp();
       for (int j = 0; j < cnt; ++j) {
+        const float4 ea = sm[j].a, eb = sm[j].b, ec = sm[j].c, ed = sm[j].d;
         const uint32_t pos = lo + uint32_t(j);
-        bool act = inside && pos >= last && S.x0[j] <= fx && fx <= S.x1[j] && S.y0[j] <= fy && fy <= S.y1[j];
         float gpx = 0.f, gpy = 0.f, gA = 0.f, gB = 0.f, gC = 0.f, gop = 0.f, gr = 0.f, gg = 0.f, gb = 0.f;
-        if (act) {
-          const float A = S.a[j], B = S.b[j], C = S.c[j], op = S.op[j];
-          const float dx = fs(fx, S.px[j]);
-          const float dy = fs(fy, S.py[j]);
-          const float q = fa(fa(fm(fm(A, dx), dx), fm(B, fa(fm(dx, dy), fm(dy, dx)))), fm(fm(C, dy), dy));
-          const float G = dexp(fm(-0.5f, q));
-          const float ee = fm(G, op);
-          const float om = 1.f - ee;
-          Tcur = Tcur / om;
-          const float wgt = ee * Tcur;
-          const float cr = S.r[j], cg = S.g[j], cb = S.bl[j];
-          const float iom = 1.f / om;
-          const float dLde = dC0 * (cr * Tcur - acc0 * iom) + dC1 * (cg * Tcur - acc1 * iom) +
-                             dC2 * (cb * Tcur - acc2 * iom);
-          acc0 += cr * wgt;
-          acc1 += cg * wgt;
-          acc2 += cb * wgt;
-          gr = wgt * dC0;
-          gg = wgt * dC1;
-          gb = wgt * dC2;
-          gop = G * dLde;
-          const float dLdq = dLde * op * G * -0.5f;
-          gA = dLdq * dx * dx;
-          gB = dLdq * 2.f * dx * dy;
-          gC = dLdq * dy * dy;
-          gpx = -dLdq * (2.f * A * dx + 2.f * B * dy);
-          gpy = -dLdq * (2.f * B * dx + 2.f * C * dy);
+        bool any = false;
+        if (ec.y <= fx && fx <= ec.w) {
+          const float A = ea.z, B = ea.w, C = eb.x, op = eb.y;
+          const float dx = fs(fx, ea.x);
+          const float adxdx = fm(fm(A, dx), dx);
+#pragma unroll
+          for (int k = 0; k < PPL; ++k) {
+            const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
+            if (pos < last[k] || !(ec.z <= fy && fy <= ed.x)) continue;
+            any = true;
+            const float dy = fs(fy, ea.y);
+            const float q = quad(B, C, dx, dy, adxdx);
+            const float Gv = dexp(fm(-0.5f, q));
+            const float al = fm(Gv, op);
+            const float om = 1.f - al;
+            const float iom = 1.f / om;
+            Tc[k] = Tc[k] * iom;
+            const float wgt = al * Tc[k];
+            const float dLde = d0[k] * (eb.z * Tc[k] - a0[k] * iom) + d1[k] * (eb.w * Tc[k] - a1[k] * iom) +
+                               d2[k] * (ec.x * Tc[k] - a2[k] * iom);
+            a0[k] += eb.z * wgt;
+            a1[k] += eb.w * wgt;
+            a2[k] += ec.x * wgt;
+            gr += wgt * d0[k];
+            gg += wgt * d1[k];
+            gb += wgt * d2[k];
+            gop += Gv * dLde;
+            const float dLdq = dLde * op * Gv * -0.5f;
+            gA += dLdq * dx * dx;
+            gB += dLdq * 2.f * dx * dy;
+            gC += dLdq * dy * dy;
+            gpx -= dLdq * (2.f * A * dx + 2.f * B * dy);
+            gpy -= dLdq * (2.f * B * dx + 2.f * C * dy);
+          }
         }
-        if (__any_sync(0xffffffffu, act)) {
+        if (__any_sync(0xffffffffu, any)) {
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) {
             gpx += __shfl_xor_sync(0xffffffffu, gpx, o);
@@ -364,16 +341,15 @@ __global__ void __launch_bounds__(TS* TS) k_raster_bwd(const ViewBatch b, uint32
             gb += __shfl_xor_sync(0xffffffffu, gb, o);
           }
           if (lane == 0) {
-            float4* dst = gv + 3 * size_t(S.gid[j]);
+            float4* dst = gv + 3 * size_t(__float_as_uint(ed.y));
             atomicAdd(dst, make_float4(gpx, gpy, gA, gB));
             atomicAdd(dst + 1, make_float4(gC, gop, gr, gg));
             atomicAdd(reinterpret_cast<float*>(dst + 2), gb);
           }
         }
       }
-      __syncthreads();
+      __syncwarp();
     }
-    __syncthreads();
   }
 }
 
@@ -426,41 +402,7 @@ __global__ void __launch_bounds__(TS* TS) k_circle_splat_tiles(int w, int h, int
 // ---------------------------------------------------------------------------
 // host launch helpers
 // ---------------------------------------------------------------------------
-template <int TS>
-static cudaError_t launch_fwd_t(cudaStream_t st, int grid, const ViewBatch& b, uint32_t n, const float4* rec,
-                                const uint32_t* item_start, const uint32_t* idx2pnt, uint32_t* counter, float* out_rgb,
-                                float* out_T, uint32_t* out_last, const float* target, float* grad_pix,
-                                float* item_loss) {
-  constexpr int NT = TS * TS;
-  const size_t sm = size_t(kSmemFloatsPerEnt) * NT * sizeof(float);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_raster_fwd<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
-  k_raster_fwd<TS><<<grid, NT, sm, st>>>(b, n, rec, item_start, idx2pnt, counter, out_rgb, out_T, out_last, target,
-                                         grad_pix, item_loss); count_launch();
-  return cudaGetLastError();
-}
-
-template <int TS>
-static cudaError_t launch_bwd_t(cudaStream_t st, int grid, const ViewBatch& b, uint32_t n, const float4* rec,
-                                const uint32_t* item_start, const uint32_t* idx2pnt, uint32_t* counter,
-                                const float* grad_pix, const float* pix_T, const uint32_t* pix_last, float4* grad2d) {
-  constexpr int NT = TS * TS;
-  const size_t sm = size_t(kSmemFloatsPerEnt) * NT * sizeof(float);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_raster_bwd<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
-  k_raster_bwd<TS><<<grid, NT, sm, st>>>(b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T, pix_last, grad2d); count_launch();
-  return cudaGetLastError();
-}
-
-static int persistent_grid(int ts, uint32_t items) {
+static int num_sms() {
   static int sms = 0;
   if (!sms) {
     int dev = 0;
@@ -468,76 +410,120 @@ static int persistent_grid(int ts, uint32_t items) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (sms <= 0) sms = 148;
   }
-  const int per_sm = ts == 8 ? 16 : (ts == 16 ? 4 : 1);
-  int g = sms * per_sm;
-  if (uint32_t(g) > items) g = int(items);
+  return sms;
+}
+
+uint32_t raster_slabs_per_tile(int ts) { return ts == 32 ? 4u : 1u; }
+
+template <class K>
+static int persistent_grid(K kernel, uint32_t tasks) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * kRasterWarps, 0);
+  if (per_sm <= 0) per_sm = 4;
+  int g = num_sms() * per_sm;
+  const uint32_t ctas = (tasks + kRasterWarps - 1) / kRasterWarps;
+  if (uint32_t(g) > ctas) g = int(ctas);
   return g < 1 ? 1 : g;
+}
+
+template <int TS>
+static void launch_fwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint32_t* item_start,
+                       const uint32_t* idx2pnt, uint32_t* counter, float* out_rgb, float* out_T, uint32_t* out_last,
+                       const float* target, float* grad_pix, float* slab_loss) {
+  static int grid_per_task = 0;  // cached occupancy-derived grid
+  static uint32_t cached_tasks = 0;
+  const uint32_t tasks = b.num_items * Geo<TS>::SLABS;
+  if (!grid_per_task || cached_tasks != tasks) {
+    grid_per_task = persistent_grid(k_raster_fwd<TS>, tasks);
+    cached_tasks = tasks;
+  }
+  k_raster_fwd<TS><<<grid_per_task, 32 * kRasterWarps, 0, st>>>(b, n, rec, item_start, idx2pnt, counter, out_rgb,
+                                                                out_T, out_last, target, grad_pix, slab_loss);
+  count_launch();
+}
+
+template <int TS>
+static void launch_bwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint32_t* item_start,
+                       const uint32_t* idx2pnt, uint32_t* counter, const float* grad_pix, const float* pix_T,
+                       const uint32_t* pix_last, float4* grad2d) {
+  static int grid = 0;
+  static uint32_t cached_tasks = 0;
+  const uint32_t tasks = b.num_items * Geo<TS>::SLABS;
+  if (!grid || cached_tasks != tasks) {
+    grid = persistent_grid(k_raster_bwd<TS>, tasks);
+    cached_tasks = tasks;
+  }
+  k_raster_bwd<TS><<<grid, 32 * kRasterWarps, 0, st>>>(b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T,
+                                                       pix_last, grad2d);
+  count_launch();
 }
 
 cudaError_t raster_fwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint32_t* item_start,
                        const uint32_t* idx2pnt, uint32_t* counter, float* out_rgb, float* out_T, uint32_t* out_last,
-                       const float* target, float* grad_pix, float* item_loss) {
-  const int grid = persistent_grid(b.ts, b.num_items);
+                       const float* target, float* grad_pix, float* slab_loss) {
   switch (b.ts) {
     case 8:
-      return launch_fwd_t<8>(st, grid, b, n, rec, item_start, idx2pnt, counter, out_rgb, out_T, out_last, target,
-                             grad_pix, item_loss);
+      launch_fwd<8>(st, b, n, rec, item_start, idx2pnt, counter, out_rgb, out_T, out_last, target, grad_pix, slab_loss);
+      break;
     case 16:
-      return launch_fwd_t<16>(st, grid, b, n, rec, item_start, idx2pnt, counter, out_rgb, out_T, out_last, target,
-                              grad_pix, item_loss);
+      launch_fwd<16>(st, b, n, rec, item_start, idx2pnt, counter, out_rgb, out_T, out_last, target, grad_pix,
+                     slab_loss);
+      break;
     case 32:
-      return launch_fwd_t<32>(st, grid, b, n, rec, item_start, idx2pnt, counter, out_rgb, out_T, out_last, target,
-                              grad_pix, item_loss);
+      launch_fwd<32>(st, b, n, rec, item_start, idx2pnt, counter, out_rgb, out_T, out_last, target, grad_pix,
+                     slab_loss);
+      break;
+    default:
+      return cudaErrorInvalidValue;
   }
-  return cudaErrorInvalidValue;
+  return cudaGetLastError();
 }
 
 cudaError_t raster_bwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint32_t* item_start,
                        const uint32_t* idx2pnt, uint32_t* counter, const float* grad_pix, const float* pix_T,
                        const uint32_t* pix_last, float4* grad2d) {
-  const int grid = persistent_grid(b.ts, b.num_items);
   switch (b.ts) {
     case 8:
-      return launch_bwd_t<8>(st, grid, b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T, pix_last, grad2d);
+      launch_bwd<8>(st, b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T, pix_last, grad2d);
+      break;
     case 16:
-      return launch_bwd_t<16>(st, grid, b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T, pix_last, grad2d);
+      launch_bwd<16>(st, b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T, pix_last, grad2d);
+      break;
     case 32:
-      return launch_bwd_t<32>(st, grid, b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T, pix_last, grad2d);
+      launch_bwd<32>(st, b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T, pix_last, grad2d);
+      break;
+    default:
+      return cudaErrorInvalidValue;
   }
-  return cudaErrorInvalidValue;
-}
-
-template <int TS>
-static cudaError_t launch_aos_t(cudaStream_t st, int w, int h, float* pix2rgb, const float* xyd, const float* conic,
-                                const float* aabb, const float* opacity, const float* rgb, const uint32_t* tile2idx,
-                                const uint32_t* idx2pnt, float* out_T, uint32_t* out_last) {
-  constexpr int NT = TS * TS;
-  const int tw = (w + TS - 1) / TS, th = (h + TS - 1) / TS;
-  if (tw == 0 || th == 0) return cudaSuccess;
-  const size_t sm = size_t(kSmemFloatsPerEnt) * NT * sizeof(float);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_raster_fwd_aos<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
-  k_raster_fwd_aos<TS><<<dim3(tw, th), NT, sm, st>>>(w, h, tw, pix2rgb, xyd, conic, aabb, opacity, rgb, tile2idx,
-                                                     idx2pnt, out_T, out_last); count_launch();
   return cudaGetLastError();
 }
 
 cudaError_t raster_fwd_aos(cudaStream_t st, int ts, int w, int h, float* pix2rgb, const float* xyd, const float* conic,
                            const float* aabb, const float* opacity, const float* rgb, const uint32_t* tile2idx,
                            const uint32_t* idx2pnt, float* out_T, uint32_t* out_last) {
+  const int tw = (w + ts - 1) / ts, th = (h + ts - 1) / ts;
+  if (tw == 0 || th == 0) return cudaSuccess;
+  const uint32_t tasks = uint32_t(tw) * uint32_t(th) * raster_slabs_per_tile(ts);
+  const unsigned grid = (tasks + kRasterWarps - 1) / kRasterWarps;
+  AosSrc src{xyd, conic, aabb, opacity, rgb};
   switch (ts) {
     case 8:
-      return launch_aos_t<8>(st, w, h, pix2rgb, xyd, conic, aabb, opacity, rgb, tile2idx, idx2pnt, out_T, out_last);
+      k_raster_fwd_aos<8><<<grid, 32 * kRasterWarps, 0, st>>>(w, h, tw, tasks, pix2rgb, src, tile2idx, idx2pnt, out_T,
+                                                              out_last);
+      break;
     case 16:
-      return launch_aos_t<16>(st, w, h, pix2rgb, xyd, conic, aabb, opacity, rgb, tile2idx, idx2pnt, out_T, out_last);
+      k_raster_fwd_aos<16><<<grid, 32 * kRasterWarps, 0, st>>>(w, h, tw, tasks, pix2rgb, src, tile2idx, idx2pnt, out_T,
+                                                               out_last);
+      break;
     case 32:
-      return launch_aos_t<32>(st, w, h, pix2rgb, xyd, conic, aabb, opacity, rgb, tile2idx, idx2pnt, out_T, out_last);
+      k_raster_fwd_aos<32><<<grid, 32 * kRasterWarps, 0, st>>>(w, h, tw, tasks, pix2rgb, src, tile2idx, idx2pnt, out_T,
+                                                               out_last);
+      break;
+    default:
+      return cudaErrorInvalidValue;
   }
-  return cudaErrorInvalidValue;
+  count_launch();
+  return cudaGetLastError();
 }
 
 cudaError_t circle_splat_tiles(cudaStream_t st, int ts, int w, int h, float* pix2rgb, const float* xyd,
@@ -546,17 +532,18 @@ cudaError_t circle_splat_tiles(cudaStream_t st, int ts, int w, int h, float* pix
   if (tw == 0 || th == 0) return cudaSuccess;
   switch (ts) {
     case 8:
-      k_circle_splat_tiles<8><<<dim3(tw, th), 64, 0, st>>>(w, h, tw, pix2rgb, xyd, rad, rgb, tile2idx, idx2pnt); count_launch();
+      k_circle_splat_tiles<8><<<dim3(tw, th), 64, 0, st>>>(w, h, tw, pix2rgb, xyd, rad, rgb, tile2idx, idx2pnt);
       break;
     case 16:
-      k_circle_splat_tiles<16><<<dim3(tw, th), 256, 0, st>>>(w, h, tw, pix2rgb, xyd, rad, rgb, tile2idx, idx2pnt); count_launch();
+      k_circle_splat_tiles<16><<<dim3(tw, th), 256, 0, st>>>(w, h, tw, pix2rgb, xyd, rad, rgb, tile2idx, idx2pnt);
       break;
     case 32:
-      k_circle_splat_tiles<32><<<dim3(tw, th), 1024, 0, st>>>(w, h, tw, pix2rgb, xyd, rad, rgb, tile2idx, idx2pnt); count_launch();
+      k_circle_splat_tiles<32><<<dim3(tw, th), 1024, 0, st>>>(w, h, tw, pix2rgb, xyd, rad, rgb, tile2idx, idx2pnt);
       break;
     default:
       return cudaErrorInvalidValue;
   }
+  count_launch();
   return cudaGetLastError();
 }
 

@@ -256,7 +256,7 @@ cudaError_t radix_sort(cudaStream_t st, uint32_t* ka, uint32_t* va, uint32_t* kb
 }
 
 // ---------------------------------------------------------------------------
-// Pair emission in rank order.
+// Rank order helpers
 // ---------------------------------------------------------------------------
 __global__ void k_iota_pad(uint32_t* __restrict__ vals, uint32_t* __restrict__ keys, uint32_t n, uint32_t npad,
                            uint32_t nseg) {
@@ -267,80 +267,283 @@ __global__ void k_iota_pad(uint32_t* __restrict__ vals, uint32_t* __restrict__ k
   if (r >= n) keys[i] = 0xffffffffu;
 }
 
-// counts in rank order: cs[v*npad + r] = cnt[v*n + order[v*npad + r]]
-__global__ void k_gather_counts(const uint32_t* __restrict__ order, const uint32_t* __restrict__ cnt, uint32_t n,
-                                uint32_t npad, uint32_t nseg, uint32_t* __restrict__ cs) {
-  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i > size_t(npad) * nseg) return;
-  if (i == size_t(npad) * nseg) {
-    cs[i] = 0;
-    return;
-  }
-  const uint32_t v = uint32_t(i / npad);
-  const uint32_t g = order[i];
-  cs[i] = g < n ? cnt[size_t(v) * n + g] : 0u;
-}
-
-__global__ void k_emit_pairs(const uint32_t* __restrict__ order, const uint32_t* __restrict__ cs,
-                             const uint32_t* __restrict__ off, const uint2* __restrict__ rect, uint32_t n,
-                             uint32_t npad, uint32_t nseg, const ViewBatch b, uint64_t capacity,
-                             uint32_t* __restrict__ pkey, uint32_t* __restrict__ pval, uint32_t* __restrict__ flags) {
-  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= size_t(npad) * nseg) return;
-  const uint32_t c = cs[i];
-  if (c == 0) return;
-  const uint32_t v = uint32_t(i / npad);
-  const uint32_t g = order[i];
-  const uint64_t o = off[i];
-  if (o + c > capacity) {
-    set_flag(flags, kFlagPairOverflow);
-    for (uint64_t j = o; j < capacity; ++j) pkey[j] = 0xffffffffu;
-    return;
-  }
-  const uint2 rc = rect[size_t(v) * n + g];
+// superblock span of a tile span (8x8 tiles per superblock); empty if no tile
+__device__ __forceinline__ bool sb_span(uint2 rc, int* sx0, int* sy0, int* sx1, int* sy1) {
   const int x0 = rc.x & 0xffff, y0 = rc.x >> 16, x1 = rc.y & 0xffff, y1 = rc.y >> 16;
-  const uint32_t tw = uint32_t(b.v[v].tile_w), base = b.v[v].item_base;
-  uint32_t j = uint32_t(o);
-  // tile_acceleration.h:34-50 order: ix outer, iy inner
-  for (int ix = x0; ix < x1; ++ix)
-    for (int iy = y0; iy < y1; ++iy) {
-      pkey[j] = base + uint32_t(iy) * tw + uint32_t(ix);
-      pval[j] = g;
-      ++j;
-    }
+  if (x1 <= x0 || y1 <= y0) return false;
+  *sx0 = x0 >> 3;
+  *sy0 = y0 >> 3;
+  *sx1 = ((x1 - 1) >> 3) + 1;
+  *sy1 = ((y1 - 1) >> 3) + 1;
+  return true;
 }
 
-// item_start[j] for j in [0, I] from the tile-sorted keys (boundary detection;
-// empty items take the start of the next non-empty one).  Keys >= I (overflow
-// sentinels) count as I.
-__global__ void k_item_ranges(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ count_ptr,
-                              uint64_t capacity, uint32_t num_items, uint32_t* __restrict__ item_start) {
-  uint32_t cnt = *count_ptr;
-  if (cnt > capacity) cnt = uint32_t(capacity);
-  auto eff = [&](size_t q) -> int64_t {
-    const uint32_t k = keys[q];
-    return k < num_items ? int64_t(k) : int64_t(num_items);
-  };
-  for (size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p <= cnt; p += size_t(gridDim.x) * blockDim.x) {
-    const int64_t k = p < cnt ? eff(p) : int64_t(num_items);
-    const int64_t kp = p > 0 ? eff(p - 1) : -1;
-    for (int64_t j = kp + 1; j <= k; ++j) item_start[j] = uint32_t(p);
+constexpr int kMsThreads = 256;
+constexpr int kMsWarps = kMsThreads / 32;
+constexpr int kMsRounds = 16;
+constexpr int kMsChunk = kMsThreads * kMsRounds;  // 4096 ranks per chunk
+
+// ---------------------------------------------------------------------------
+// Stage 1a: per (chunk, superblock) counts.  Block = one chunk of 4096 ranks
+// of one view.  Output layout cnt[(sb_base[v] + s) * nchunk + c] so that an
+// exclusive scan in index order yields (view, superblock, rank) positions.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restrict__ order,
+                                                         const uint2* __restrict__ rect, uint32_t n, uint32_t npad,
+                                                         const ViewBatch b,
+                                                         uint32_t* __restrict__ cnt) {
+  extern __shared__ uint32_t hist[];
+  const uint32_t nchunk = npad / kMsChunk;
+  const uint32_t v = blockIdx.x / nchunk, c = blockIdx.x % nchunk;
+  const ViewDev& vd = b.v[v];
+  const int sbw = (vd.tile_w + 7) >> 3, sbh = (vd.tile_h + 7) >> 3;
+  const int nsb = sbw * sbh;
+  for (int i = threadIdx.x; i < nsb; i += kMsThreads) hist[i] = 0;
+  __syncthreads();
+  const size_t base = size_t(v) * npad + size_t(c) * kMsChunk;
+  for (int i = threadIdx.x; i < kMsChunk; i += kMsThreads) {
+    const uint32_t g = order[base + i];
+    if (g >= n) continue;
+    int sx0, sy0, sx1, sy1;
+    if (!sb_span(rect[size_t(v) * n + g], &sx0, &sy0, &sx1, &sy1)) continue;
+    for (int sy = sy0; sy < sy1; ++sy)
+      for (int sx = sx0; sx < sx1; ++sx) atomicAdd(&hist[sy * sbw + sx], 1u);
   }
+  __syncthreads();
+  const uint32_t sb0 = vd.sb_base;
+  for (int i = threadIdx.x; i < nsb; i += kMsThreads) cnt[(size_t(sb0) + i) * nchunk + c] = hist[i];
+}
+
+// ---------------------------------------------------------------------------
+// Stage 1b: stable scatter of point indices into superblock lists.  Warp w
+// owns ranks [w*512, w*512+512) of the chunk in 16 rounds of 32; inside a
+// round a lane's rank among the lanes that hit the same superblock is counted
+// from the other lanes' spans (fetched by shuffle).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void lane_rank(const uint32_t* spans, int lane, int sx, int sy, int* below, int* above) {
+  int bl = 0, ab = 0;
+#pragma unroll
+  for (int l = 0; l < 32; ++l) {
+    const uint32_t p = spans[l];
+    const int ax0 = p & 255, ay0 = (p >> 8) & 255, ax1 = (p >> 16) & 255, ay1 = p >> 24;
+    const bool in = sx >= ax0 && sx < ax1 && sy >= ay0 && sy < ay1;
+    bl += (in && l < lane);
+    ab += (in && l > lane);
+  }
+  *below = bl;
+  *above = ab;
+}
+
+__global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __restrict__ order,
+                                                           const uint2* __restrict__ rect, uint32_t n, uint32_t npad,
+                                                           const ViewBatch b,
+                                                           const uint32_t* __restrict__ off, uint64_t capacity,
+                                                           uint32_t* __restrict__ list1, uint32_t* __restrict__ flags) {
+  extern __shared__ uint32_t wc[];  // [kMsWarps][nsb]
+  const uint32_t nchunk = npad / kMsChunk;
+  const uint32_t v = blockIdx.x / nchunk, c = blockIdx.x % nchunk;
+  const ViewDev& vd = b.v[v];
+  const int sbw = (vd.tile_w + 7) >> 3, sbh = (vd.tile_h + 7) >> 3;
+  const int nsb = sbw * sbh;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < kMsWarps * nsb; i += kMsThreads) wc[i] = 0;
+  __syncthreads();
+  const size_t base = size_t(v) * npad + size_t(c) * kMsChunk + size_t(warp) * (kMsRounds * 32);
+  uint32_t* my = wc + warp * nsb;
+  // phase 1: per-warp counts
+  for (int r = 0; r < kMsRounds; ++r) {
+    const uint32_t g = order[base + r * 32 + lane];
+    int sx0, sy0, sx1, sy1;
+    if (g < n && sb_span(rect[size_t(v) * n + g], &sx0, &sy0, &sx1, &sy1))
+      for (int sy = sy0; sy < sy1; ++sy)
+        for (int sx = sx0; sx < sx1; ++sx) atomicAdd(&my[sy * sbw + sx], 1u);
+  }
+  __syncthreads();
+  // phase 2: warp bases = chunk offset + earlier warps
+  const uint32_t sb0 = vd.sb_base;
+  for (int i = threadIdx.x; i < nsb; i += kMsThreads) {
+    uint32_t run = off[(size_t(sb0) + i) * nchunk + c];
+    for (int w = 0; w < kMsWarps; ++w) {
+      const uint32_t t = wc[w * nsb + i];
+      wc[w * nsb + i] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+  // phase 3: stable scatter, round by round
+  uint32_t spans[32];
+  for (int r = 0; r < kMsRounds; ++r) {
+    const uint32_t g = order[base + r * 32 + lane];
+    int sx0 = 0, sy0 = 0, sx1 = 0, sy1 = 0;
+    const bool has = g < n && sb_span(rect[size_t(v) * n + g], &sx0, &sy0, &sx1, &sy1);
+    const uint32_t packed =
+        has ? (uint32_t(sx0) | uint32_t(sy0) << 8 | uint32_t(sx1) << 16 | uint32_t(sy1) << 24) : 0u;
+#pragma unroll
+    for (int l = 0; l < 32; ++l) spans[l] = __shfl_sync(0xffffffffu, packed, l);
+    for (int sy = sy0; sy < sy1; ++sy)
+      for (int sx = sx0; sx < sx1; ++sx) {
+        int below, above;
+        lane_rank(spans, lane, sx, sy, &below, &above);
+        const uint32_t dst = my[sy * sbw + sx] + uint32_t(below);
+        if (dst < capacity) list1[dst] = g;
+        else set_flag(flags, kFlagPairOverflow);
+      }
+    __syncwarp();
+    // the highest lane hitting a superblock advances the warp's counter
+    for (int sy = sy0; sy < sy1; ++sy)
+      for (int sx = sx0; sx < sx1; ++sx) {
+        int below, above;
+        lane_rank(spans, lane, sx, sy, &below, &above);
+        if (above == 0) my[sy * sbw + sx] += uint32_t(below + 1);
+      }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stage 2a: per-tile pair counts, one CTA per superblock walking its list.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int view_of_sb(const ViewBatch& b, uint32_t sb) {
+  int v = 0;
+  for (int k = 1; k < b.num_views; ++k)
+    if (sb >= b.v[k].sb_base) v = k;
+  return v;
+}
+
+__global__ void __launch_bounds__(kMsThreads) k_tile_count(const uint32_t* __restrict__ list1,
+                                                           const uint32_t* __restrict__ off1, uint32_t nchunk,
+                                                           uint64_t capacity, const uint2* __restrict__ rect,
+                                                           uint32_t n, const ViewBatch b,
+                                                           uint32_t* __restrict__ tcnt) {
+  __shared__ uint32_t h[64];
+  const uint32_t sb = blockIdx.x;
+  const int v = view_of_sb(b, sb);
+  const ViewDev& vd = b.v[v];
+  const int sbw = (vd.tile_w + 7) >> 3;
+  const uint32_t ls = sb - vd.sb_base;
+  const int tx0 = int(ls % uint32_t(sbw)) * 8, ty0 = int(ls / uint32_t(sbw)) * 8;
+  if (threadIdx.x < 64) h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint64_t s = min(uint64_t(off1[size_t(sb) * nchunk]), capacity);
+  const uint64_t e = min(uint64_t(off1[size_t(sb + 1) * nchunk]), capacity);
+  for (uint64_t i = s + threadIdx.x; i < e; i += kMsThreads) {
+    const uint2 rc = rect[size_t(v) * n + list1[i]];
+    const int x0 = max(int(rc.x & 0xffff), tx0), x1 = min(int(rc.y & 0xffff), tx0 + 8);
+    const int y0 = max(int(rc.x >> 16), ty0), y1 = min(int(rc.y >> 16), ty0 + 8);
+    for (int y = y0; y < y1; ++y)
+      for (int x = x0; x < x1; ++x) atomicAdd(&h[(y - ty0) * 8 + (x - tx0)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 64) {
+    const int x = tx0 + (threadIdx.x & 7), y = ty0 + (threadIdx.x >> 3);
+    if (x < vd.tile_w && y < vd.tile_h) tcnt[vd.item_base + uint32_t(y) * vd.tile_w + x] = h[threadIdx.x];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stage 2b: stable scatter into tile lists.  Chunks of 256 list entries, one
+// per thread in order; for each of the 64 tiles a warp ballot says which lanes
+// cover it, and popcounts of the ballots give every pair its slot:
+//   slot = tile start + earlier chunks + earlier warps + lower lanes.
+// out_tile (nullable) receives each pair's item id.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kMsThreads) k_tile_scatter(const uint32_t* __restrict__ list1,
+                                                             const uint32_t* __restrict__ off1, uint32_t nchunk,
+                                                             uint64_t capacity, const uint2* __restrict__ rect,
+                                                             uint32_t n, const ViewBatch b,
+                                                               const uint32_t* __restrict__ item_start,
+                                                             uint32_t* __restrict__ idx2pnt,
+                                                             uint32_t* __restrict__ out_tile,
+                                                             uint32_t* __restrict__ flags) {
+  __shared__ uint32_t run[64];
+  __shared__ uint32_t tot[64];
+  __shared__ uint32_t masks[kMsWarps][64];
+  __shared__ uint32_t pre[kMsWarps][64];
+  const uint32_t sb = blockIdx.x;
+  const int v = view_of_sb(b, sb);
+  const ViewDev& vd = b.v[v];
+  const int sbw = (vd.tile_w + 7) >> 3;
+  const uint32_t ls = sb - vd.sb_base;
+  const int tx0 = int(ls % uint32_t(sbw)) * 8, ty0 = int(ls / uint32_t(sbw)) * 8;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  if (threadIdx.x < 64) {
+    const int x = tx0 + (threadIdx.x & 7), y = ty0 + (threadIdx.x >> 3);
+    run[threadIdx.x] = (x < vd.tile_w && y < vd.tile_h) ? item_start[vd.item_base + uint32_t(y) * vd.tile_w + x] : 0u;
+  }
+  __syncthreads();
+  const uint64_t s = min(uint64_t(off1[size_t(sb) * nchunk]), capacity);
+  const uint64_t e = min(uint64_t(off1[size_t(sb + 1) * nchunk]), capacity);
+  for (uint64_t c0 = s; c0 < e; c0 += kMsThreads) {
+    const uint64_t i = c0 + threadIdx.x;
+    uint32_t g = 0;
+    int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
+    if (i < e) {
+      g = list1[i];
+      const uint2 rc = rect[size_t(v) * n + g];
+      x0 = max(int(rc.x & 0xffff), tx0) - tx0;
+      x1 = min(int(rc.y & 0xffff), tx0 + 8) - tx0;
+      y0 = max(int(rc.x >> 16), ty0) - ty0;
+      y1 = min(int(rc.y >> 16), ty0 + 8) - ty0;
+    }
+#pragma unroll
+    for (int k = 0; k < 64; ++k) {
+      const int kx = k & 7, ky = k >> 3;
+      const uint32_t m = __ballot_sync(0xffffffffu, kx >= x0 && kx < x1 && ky >= y0 && ky < y1);
+      if ((k & 31) == lane) masks[warp][k] = m;
+    }
+    __syncthreads();
+    if (threadIdx.x < 64) {
+      uint32_t acc = 0;
+#pragma unroll
+      for (int w = 0; w < kMsWarps; ++w) {
+        pre[w][threadIdx.x] = acc;
+        acc += __popc(masks[w][threadIdx.x]);
+      }
+      tot[threadIdx.x] = acc;
+    }
+    __syncthreads();
+    for (int y = y0; y < y1; ++y)
+      for (int x = x0; x < x1; ++x) {
+        const int k = y * 8 + x;
+        const uint32_t slot = run[k] + pre[warp][k] + __popc(masks[warp][k] & lt);
+        if (slot < capacity) {
+          idx2pnt[slot] = g;
+          if (out_tile) out_tile[slot] = vd.item_base + uint32_t(ty0 + y) * vd.tile_w + uint32_t(tx0 + x);
+        } else {
+          set_flag(flags, kFlagPairOverflow);
+        }
+      }
+    __syncthreads();
+    if (threadIdx.x < 64) run[threadIdx.x] += tot[threadIdx.x];
+    __syncthreads();
+  }
+}
+
+// Clamp tile ranges to the pair capacity after an overflow so that readers
+// stay in bounds (the results are then invalid and the flag is set).
+__global__ void k_clamp_ranges(uint32_t* __restrict__ item_start, uint32_t num_items, uint64_t capacity,
+                               uint32_t* __restrict__ flags) {
+  const uint32_t total = item_start[num_items];
+  if (total <= capacity) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) set_flag(flags, kFlagPairOverflow);
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i <= num_items; i += size_t(gridDim.x) * blockDim.x)
+    if (item_start[i] > capacity) item_start[i] = uint32_t(capacity);
 }
 
 __global__ void k_copy_total(const uint32_t* __restrict__ off, size_t idx, uint32_t* __restrict__ out) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *out = off[idx];
 }
 
-// keys for the drop-in API: idx2tiledepth = (tile << 32) | depth bits, the
-// depth bits recomputed from pnt2pixxydepth (the key buffer is sorted by now)
-__global__ void k_make_keys64(const uint32_t* __restrict__ tkey, const uint32_t* __restrict__ tval,
+// keys for the drop-in API: idx2tiledepth = (tile << 32) | depth bits of the
+// point, recomputed from pnt2pixxydepth
+__global__ void k_make_keys64(const uint32_t* __restrict__ tile, const uint32_t* __restrict__ pnt,
                               const float* __restrict__ xyd, const uint32_t* __restrict__ count_ptr,
                               uint64_t capacity, uint64_t* __restrict__ out) {
   uint32_t cnt = *count_ptr;
   if (cnt > capacity) cnt = uint32_t(capacity);
   for (size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p < cnt; p += size_t(gridDim.x) * blockDim.x)
-    out[p] = (uint64_t(tkey[p]) << 32) | depth_bits(xyd[3 * size_t(tval[p]) + 2]);
+    out[p] = (uint64_t(tile[p]) << 32) | depth_bits(xyd[3 * size_t(pnt[p]) + 2]);
 }
 
 }  // namespace dsplat

@@ -50,11 +50,11 @@ class GaussGrads(ctypes.Structure):
 
 class BatchLayout(ctypes.Structure):
     _fields_ = [("total_bytes", c_size), ("num_items", c_u32), ("num_pix", c_u32), ("npad", c_u32),
-                ("tile_sort_bits", c_u32),
+                ("slabs_per_tile", c_u32),
                 ("off_flags", c_size), ("off_rec", c_size), ("off_rect", c_size), ("off_cnt", c_size),
                 ("off_order", c_size), ("off_item_start", c_size), ("off_idx2pnt", c_size),
-                ("off_item_key", c_size), ("off_pix_T", c_size), ("off_pix_stop", c_size),
-                ("off_grad_pix", c_size), ("off_item_loss", c_size), ("off_grad2d", c_size)]
+                ("off_sb_list", c_size), ("off_pix_T", c_size), ("off_pix_stop", c_size),
+                ("off_grad_pix", c_size), ("off_slab_loss", c_size), ("off_grad2d", c_size)]
 
 
 _P = c_void_p  # every pointer is passed as an integer address

@@ -164,8 +164,10 @@ class GaussBatch:
         p0, p1 = int(s[0]), int(s[-1])
         return (s - p0).to(torch.int32), idx[p0:p1]
 
-    def item_loss(self) -> torch.Tensor:
-        return self._ws(self.layout.off_item_loss, int(self.layout.num_items), torch.float32)
+    def slab_loss(self) -> torch.Tensor:
+        """Partial L2 losses of the last forward with a target (sum = loss)."""
+        L = self.layout
+        return self._ws(L.off_slab_loss, int(L.num_items) * int(L.slabs_per_tile), torch.float32)
 
     def grad2d(self) -> torch.Tensor:
         return self._ws(self.layout.off_grad2d, self.num_views * self.n * 12, torch.float32).view(

@@ -164,7 +164,7 @@ typedef struct {
   uint32_t num_items; /* sum over views of tiles */
   uint32_t num_pix;   /* sum over views of pixels */
   uint32_t npad;      /* per-view padded point count of the depth sort */
-  uint32_t tile_sort_bits;
+  uint32_t slabs_per_tile; /* raster warp tasks per tile (4 for 32x32 tiles, else 1) */
   size_t off_flags;      /* u32[4]: flags, total pairs, counters */
   size_t off_rec;        /* float4[V*N*3] per-view 2D records */
   size_t off_rect;       /* uint2[V*N] tile spans */
@@ -172,11 +172,11 @@ typedef struct {
   size_t off_order;      /* u32[V*npad] points in depth order per view */
   size_t off_item_start; /* u32[num_items+1] */
   size_t off_idx2pnt;    /* u32[capacity] points sorted by (item, depth) */
-  size_t off_item_key;   /* u32[capacity] item id of each sorted pair */
+  size_t off_sb_list;    /* u32[capacity] stage-1 superblock lists */
   size_t off_pix_T;      /* f32[num_pix] final transmittance */
   size_t off_pix_stop;   /* u32[num_pix] list position where the walk stopped */
   size_t off_grad_pix;   /* f32[num_pix*3] dL/dpixel (loss gradient) */
-  size_t off_item_loss;  /* f32[num_items] per-item partial L2 loss */
+  size_t off_slab_loss;  /* f32[num_items*slabs_per_tile] partial L2 losses */
   size_t off_grad2d;     /* float4[V*N*3] per-view 2D gradients */
 } dsplat_batch_layout;
 
