@@ -22,7 +22,7 @@ __global__ void k_project_bwd(uint32_t, int, const float*, const float*, const f
                               const float4*, float*, float*, float*, float*, float*);
 __global__ void k_adam(size_t, float*, const float*, float*, float*, float, float, float, float, float, float);
 __global__ void k_iota_pad(uint32_t*, uint32_t*, uint32_t, uint32_t, uint32_t);
-__global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*);
+__global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*, uint32_t*);
 __global__ void k_sb_scatter(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
                              uint64_t, uint32_t*, uint32_t*);
 __global__ void k_tile_count(const uint32_t*, const uint32_t*, uint32_t, uint64_t, const uint2*, uint32_t,
@@ -148,7 +148,7 @@ int build_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npad, 
     if (smem3 > 200 * 1024) return fail(DSPLAT_ERR_UNSUPPORTED, "too many superblocks in one view");
     TRY_CUDA(cudaFuncSetAttribute(k_sb_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)), "attr");
   }
-  k_sb_count<<<grid1, 256, smem1, st>>>(order, rect, n, npad, b, L.cnt1);
+  k_sb_count<<<grid1, 256, smem1, st>>>(order, rect, n, npad, b, L.cnt1, flags + 1);
   count_launch();
   TRY_CUDA(cudaMemsetAsync(L.cnt1 + m, 0, sizeof(uint32_t), st), "memset");
   TRY_CUDA(exclusive_scan(st, L.cnt1, L.off1, m + 1, scan_tmp), "scan");
@@ -158,8 +158,6 @@ int build_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npad, 
   k_tile_count<<<b.num_sb, 256, 0, st>>>(L.list1, L.off1, nchunk, capacity, rect, n, b, L.tcnt);
   count_launch();
   TRY_CUDA(exclusive_scan(st, L.tcnt, item_start, size_t(b.num_items) + 1, scan_tmp), "scan");
-  k_copy_total<<<1, 32, 0, st>>>(item_start, b.num_items, flags + 1);
-  count_launch();
   k_tile_scatter<<<b.num_sb, 256, 0, st>>>(L.list1, L.off1, nchunk, capacity, rect, n, b, item_start, idx2pnt,
                                            out_tile, flags);
   count_launch();

@@ -291,7 +291,8 @@ constexpr int kMsChunk = kMsThreads * kMsRounds;  // 4096 ranks per chunk
 __global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restrict__ order,
                                                          const uint2* __restrict__ rect, uint32_t n, uint32_t npad,
                                                          const ViewBatch b,
-                                                         uint32_t* __restrict__ cnt) {
+                                                         uint32_t* __restrict__ cnt,
+                                                         uint32_t* __restrict__ total_pairs) {
   extern __shared__ uint32_t hist[];
   const uint32_t nchunk = npad / kMsChunk;
   const uint32_t v = blockIdx.x / nchunk, c = blockIdx.x % nchunk;
@@ -301,14 +302,21 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restr
   for (int i = threadIdx.x; i < nsb; i += kMsThreads) hist[i] = 0;
   __syncthreads();
   const size_t base = size_t(v) * npad + size_t(c) * kMsChunk;
+  uint32_t pairs = 0;
   for (int i = threadIdx.x; i < kMsChunk; i += kMsThreads) {
     const uint32_t g = order[base + i];
     if (g >= n) continue;
+    const uint2 rc = rect[size_t(v) * n + g];
     int sx0, sy0, sx1, sy1;
-    if (!sb_span(rect[size_t(v) * n + g], &sx0, &sy0, &sx1, &sy1)) continue;
+    if (!sb_span(rc, &sx0, &sy0, &sx1, &sy1)) continue;
+    pairs += uint32_t((rc.y & 0xffff) - (rc.x & 0xffff)) * uint32_t((rc.y >> 16) - (rc.x >> 16));
     for (int sy = sy0; sy < sy1; ++sy)
       for (int sx = sx0; sx < sx1; ++sx) atomicAdd(&hist[sy * sbw + sx], 1u);
   }
+  // exact pair total (tile-span areas), known even when a later stage overflows
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+  if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(total_pairs, pairs);
   __syncthreads();
   const uint32_t sb0 = vd.sb_base;
   for (int i = threadIdx.x; i < nsb; i += kMsThreads) cnt[(size_t(sb0) + i) * nchunk + c] = hist[i];
