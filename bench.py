@@ -272,7 +272,7 @@ def main():
     clocks = clk.summary()
 
     # untimed check: no capacity overflow happened
-    flags, pairs_now = batch.status()
+    flags, needed_now, pairs_now = batch.status()
     if flags:
         raise RuntimeError("pair capacity overflow inside the timed region")
 

@@ -24,11 +24,10 @@ __global__ void k_adam(size_t, float*, const float*, float*, float*, float, floa
 __global__ void k_iota_pad(uint32_t*, uint32_t*, uint32_t, uint32_t, uint32_t);
 __global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*, uint32_t*);
 __global__ void k_sb_scatter(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
-                             uint64_t, uint32_t*, uint32_t*);
-__global__ void k_tile_count(const uint32_t*, const uint32_t*, uint32_t, uint64_t, const uint2*, uint32_t,
-                             const ViewBatch, uint32_t*);
-__global__ void k_tile_scatter(const uint32_t*, const uint32_t*, uint32_t, uint64_t, const uint2*, uint32_t,
-                               const ViewBatch, const uint32_t*, uint32_t*, uint32_t*, uint32_t*);
+                             uint64_t, uint2*, uint32_t*);
+__global__ void k_tile_count(const uint2*, const uint32_t*, uint32_t, uint64_t, const ViewBatch, uint32_t*);
+__global__ void k_tile_scatter(const uint2*, const uint32_t*, uint32_t, uint64_t, const ViewBatch, const uint32_t*,
+                               uint32_t*, uint32_t*, uint32_t*);
 __global__ void k_clamp_ranges(uint32_t*, uint32_t, uint64_t, uint32_t*);
 __global__ void k_copy_total(const uint32_t*, size_t, uint32_t*);
 __global__ void k_make_keys64(const uint32_t*, const uint32_t*, const float*, const uint32_t*, uint64_t, uint64_t*);
@@ -43,10 +42,10 @@ size_t radix_hist_words(size_t n);
 cudaError_t exclusive_scan(cudaStream_t, const uint32_t*, uint32_t*, size_t, uint32_t*);
 cudaError_t radix_sort(cudaStream_t, uint32_t*, uint32_t*, uint32_t*, uint32_t*, size_t, const uint32_t*, int, uint32_t,
                        uint32_t*, uint32_t*, bool*);
-cudaError_t raster_fwd(cudaStream_t, const ViewBatch&, uint32_t, const float4*, const uint32_t*, const uint32_t*,
-                       uint32_t*, float*, float*, uint32_t*, const float*, float*, float*);
-cudaError_t raster_bwd(cudaStream_t, const ViewBatch&, uint32_t, const float4*, const uint32_t*, const uint32_t*,
-                       uint32_t*, const float*, const float*, const uint32_t*, float4*);
+cudaError_t raster_fwd(cudaStream_t, const ViewBatch&, uint32_t, const float4*, const uint2*, const uint32_t*, uint32_t,
+                       uint64_t, uint32_t*, float*, float*, uint32_t*, const float*, float*, float*);
+cudaError_t raster_bwd(cudaStream_t, const ViewBatch&, uint32_t, const float4*, const uint2*, const uint32_t*, uint32_t,
+                       uint64_t, uint32_t*, const float*, const float*, const uint32_t*, float4*);
 cudaError_t raster_fwd_aos(cudaStream_t, int, int, int, float*, const float*, const float*, const float*, const float*,
                            const float*, const uint32_t*, const uint32_t*, float*, uint32_t*);
 cudaError_t circle_splat_tiles(cudaStream_t, int, int, int, float*, const float*, const float*, const float*,
@@ -120,7 +119,8 @@ struct Carver {
 constexpr uint32_t kChunk = 4096;  // ranks per stage-1 chunk (= kSortTile)
 
 struct ListsWs {
-  uint32_t *cnt1, *off1, *list1, *tcnt;
+  uint32_t *cnt1, *off1, *tcnt;
+  uint2* list1;
 };
 
 size_t lists_scan_words(const ViewBatch& b, uint32_t npad) {
@@ -128,17 +128,19 @@ size_t lists_scan_words(const ViewBatch& b, uint32_t npad) {
   return a > c ? a : c;
 }
 
-void carve_lists(Carver& c, const ViewBatch& b, uint32_t npad, size_t cap, ListsWs* L, size_t* off_list1) {
+void carve_lists(Carver& c, const ViewBatch& b, uint32_t npad, size_t cap, ListsWs* L, size_t* off_list1,
+                 size_t* off_off1) {
   const size_t m = size_t(b.num_sb) * (npad / kChunk) + 1;
   L->cnt1 = c.take<uint32_t>(m);
-  L->off1 = c.take<uint32_t>(m);
-  L->list1 = c.take<uint32_t>(cap, off_list1);
+  L->off1 = c.take<uint32_t>(m, off_off1);
+  L->list1 = c.take<uint2>(cap, off_list1);
   L->tcnt = c.take<uint32_t>(size_t(b.num_items) + 1);
 }
 
-int build_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npad, const uint32_t* order,
-                const uint2* rect, const ListsWs& L, uint32_t* scan_tmp, uint32_t* item_start, uint32_t* idx2pnt,
-                uint32_t* out_tile, uint64_t capacity, uint32_t* flags) {
+// Stage 1: superblock lists of (point, local tile span) in rank order.
+// flags[1] <- tile pairs P, flags[4] <- superblock entries (capacity needed).
+int build_sb_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npad, const uint32_t* order,
+                   const uint2* rect, const ListsWs& L, uint32_t* scan_tmp, uint64_t capacity, uint32_t* flags) {
   const uint32_t nchunk = npad / kChunk;
   const size_t m = size_t(b.num_sb) * nchunk;
   const unsigned grid1 = unsigned(b.num_views) * nchunk;
@@ -152,14 +154,25 @@ int build_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npad, 
   count_launch();
   TRY_CUDA(cudaMemsetAsync(L.cnt1 + m, 0, sizeof(uint32_t), st), "memset");
   TRY_CUDA(exclusive_scan(st, L.cnt1, L.off1, m + 1, scan_tmp), "scan");
+  k_copy_total<<<1, 32, 0, st>>>(L.off1, m, flags + 4);
+  count_launch();
   k_sb_scatter<<<grid1, 256, smem3, st>>>(order, rect, n, npad, b, L.off1, capacity, L.list1, flags);
   count_launch();
+  TRY_CUDA(cudaGetLastError(), "superblock lists");
+  return DSPLAT_OK;
+}
+
+// Stage 2 (reference-format output only): per-tile lists tile2idx/idx2pnt.
+int build_tile_lists(cudaStream_t st, const ViewBatch& b, uint32_t npad, const ListsWs& L, uint32_t* scan_tmp,
+                     uint32_t* item_start, uint32_t* idx2pnt, uint32_t* out_tile, uint64_t capacity,
+                     uint32_t* flags) {
+  const uint32_t nchunk = npad / kChunk;
   TRY_CUDA(cudaMemsetAsync(L.tcnt + b.num_items, 0, sizeof(uint32_t), st), "memset");
-  k_tile_count<<<b.num_sb, 256, 0, st>>>(L.list1, L.off1, nchunk, capacity, rect, n, b, L.tcnt);
+  k_tile_count<<<b.num_sb, 256, 0, st>>>(L.list1, L.off1, nchunk, capacity, b, L.tcnt);
   count_launch();
   TRY_CUDA(exclusive_scan(st, L.tcnt, item_start, size_t(b.num_items) + 1, scan_tmp), "scan");
-  k_tile_scatter<<<b.num_sb, 256, 0, st>>>(L.list1, L.off1, nchunk, capacity, rect, n, b, item_start, idx2pnt,
-                                           out_tile, flags);
+  k_tile_scatter<<<b.num_sb, 256, 0, st>>>(L.list1, L.off1, nchunk, capacity, b, item_start, idx2pnt, out_tile,
+                                           flags);
   count_launch();
   k_clamp_ranges<<<64, 256, 0, st>>>(item_start, b.num_items, capacity, flags);
   count_launch();
@@ -225,8 +238,8 @@ TileWs carve_tiles(void* ws, uint32_t n, uint32_t tile_w, uint32_t tile_h, uint6
   if (hw > sw) sw = hw;
   if (size_t(n) + 1 > sw) sw = size_t(n) + 1;
   t.scan_tmp = c.take<uint32_t>(scan_tmp_words(sw));
-  size_t dummy;
-  carve_lists(c, b, npad, cap, &t.lists, &dummy);
+  size_t d0, d1;
+  carve_lists(c, b, npad, cap, &t.lists, &d0, &d1);
   t.out_tile = c.take<uint32_t>(cap);
   t.bytes = c.off;
   return t;
@@ -281,8 +294,10 @@ int tiles_fill(cudaStream_t st, uint32_t n, const float* xyd, const float* aabb,
   bool in_b = false;
   TRY_CUDA(radix_sort(st, t.dka, t.dva, t.dkb, t.dvb, npad, nullptr, 32, 1, t.hist, t.scan_tmp, &in_b), "depth sort");
   const uint32_t* order = in_b ? t.dvb : t.dva;
-  int rc = build_lists(st, b, n, npad, order, t.rect, t.lists, t.scan_tmp, tile2idx, idx2pnt,
-                       keys64 ? t.out_tile : nullptr, capacity, t.flags);
+  int rc = build_sb_lists(st, b, n, npad, order, t.rect, t.lists, t.scan_tmp, capacity, t.flags);
+  if (rc) return rc;
+  rc = build_tile_lists(st, b, npad, t.lists, t.scan_tmp, tile2idx, idx2pnt, keys64 ? t.out_tile : nullptr, capacity,
+                        t.flags);
   if (rc) return rc;
   if (keys64) {
     k_make_keys64<<<1184, 256, 0, st>>>(t.out_tile, idx2pnt, xyd, t.flags + 1, capacity, keys64);
@@ -300,7 +315,7 @@ struct BatchWs {
   uint32_t* flags;
   float4* rec;
   uint2* rect;
-  uint32_t *cnt, *dka, *dva, *dkb, *dvb, *hist, *scan_tmp, *item_start, *idx2pnt;
+  uint32_t *cnt, *dka, *dva, *dkb, *dvb, *hist, *scan_tmp;
   ListsWs lists;
   float* pix_T;
   uint32_t* pix_stop;
@@ -369,9 +384,9 @@ BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity)
   size_t sw = lists_scan_words(b, npad);
   if (hw > sw) sw = hw;
   w.scan_tmp = c.take<uint32_t>(scan_tmp_words(sw));
-  carve_lists(c, b, npad, cap, &w.lists, &L.off_sb_list);
-  w.item_start = c.take<uint32_t>(size_t(b.num_items) + 1, &L.off_item_start);
-  w.idx2pnt = c.take<uint32_t>(cap, &L.off_idx2pnt);
+  carve_lists(c, b, npad, cap, &w.lists, &L.off_sb_list, &L.off_sb_start);
+  L.sb_chunks = npad / kChunk;
+  L.num_sb = b.num_sb;
   w.pix_T = c.take<float>(b.num_pix, &L.off_pix_T);
   w.pix_stop = c.take<uint32_t>(b.num_pix, &L.off_pix_stop);
   w.grad_pix = c.take<float>(size_t(b.num_pix) * 3, &L.off_grad_pix);
@@ -573,7 +588,7 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
   stage_mark(st, 0);
   TRY_CUDA(cudaMemsetAsync(w.flags, 0, 16 * sizeof(uint32_t), st), "memset");
   if (n == 0 || pair_capacity == 0) {
-    TRY_CUDA(cudaMemsetAsync(w.item_start, 0, (size_t(b.num_items) + 1) * 4, st), "memset");
+    TRY_CUDA(cudaMemsetAsync(w.lists.off1, 0, (size_t(b.num_sb) * (npad / kChunk) + 1) * 4, st), "memset");
   } else {
     k_iota_pad<<<blocks_for(Vp, 256), 256, 0, st>>>(w.dva, w.dka, n, npad, V);
     count_launch();
@@ -586,14 +601,13 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
     TRY_CUDA(radix_sort(st, w.dka, w.dva, w.dkb, w.dvb, Vp, nullptr, 32, V, w.hist, w.scan_tmp, &in_b), "depth sort");
     stage_mark(st, 2);
     const uint32_t* order = in_b ? w.dvb : w.dva;
-    int rc2 = build_lists(st, b, n, npad, order, w.rect, w.lists, w.scan_tmp, w.item_start, w.idx2pnt, nullptr,
-                          pair_capacity, w.flags);
+    int rc2 = build_sb_lists(st, b, n, npad, order, w.rect, w.lists, w.scan_tmp, pair_capacity, w.flags);
     if (rc2) return rc2;
     stage_mark(st, 3);
   }
   stage_mark(st, 4);
-  TRY_CUDA(raster_fwd(st, b, n, w.rec, w.item_start, w.idx2pnt, w.flags + 2, out_rgb, w.pix_T, w.pix_stop, target,
-                      w.grad_pix, w.slab_loss),
+  TRY_CUDA(raster_fwd(st, b, n, w.rec, w.lists.list1, w.lists.off1, npad / kChunk, pair_capacity, w.flags + 2, out_rgb,
+                      w.pix_T, w.pix_stop, target, w.grad_pix, w.slab_loss),
            "raster_fwd");
   stage_mark(st, 5);
   if (out_alpha) {
@@ -626,8 +640,8 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
   TRY_CUDA(cudaMemsetAsync(w.grad2d, 0, 3 * VN * sizeof(float4), st), "memset");
   TRY_CUDA(cudaMemsetAsync(w.flags + 3, 0, sizeof(uint32_t), st), "memset");
   stage_mark(st, 7);
-  TRY_CUDA(raster_bwd(st, b, n, w.rec, w.item_start, w.idx2pnt, w.flags + 3, grad_rgb ? grad_rgb : w.grad_pix, w.pix_T,
-                      w.pix_stop, w.grad2d),
+  TRY_CUDA(raster_bwd(st, b, n, w.rec, w.lists.list1, w.lists.off1, w.L.npad / kChunk, pair_capacity, w.flags + 3,
+                      grad_rgb ? grad_rgb : w.grad_pix, w.pix_T, w.pix_stop, w.grad2d),
            "raster_bwd");
   stage_mark(st, 8);
   k_project_bwd<<<blocks_for(n, 128), 128, 0, st>>>(n, params->sh_degree, params->means, params->log_scales,
@@ -638,14 +652,16 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
   return DSPLAT_OK;
 }
 
-int dsplat_gauss_batch_status(dsplat_stream stream, const void* workspace, uint32_t* flags, uint64_t* num_pairs) {
+int dsplat_gauss_batch_status(dsplat_stream stream, const void* workspace, uint32_t* flags, uint64_t* capacity_needed,
+                              uint64_t* tile_pairs) {
   if (!workspace) return fail(DSPLAT_ERR_INVALID_ARG, "workspace is null");
-  uint32_t h[2] = {0, 0};
+  uint32_t h[5] = {0, 0, 0, 0, 0};
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   TRY_CUDA(cudaMemcpyAsync(h, workspace, sizeof(h), cudaMemcpyDeviceToHost, st), "memcpy");
   TRY_CUDA(cudaStreamSynchronize(st), "sync");
   if (flags) *flags = h[0];
-  if (num_pairs) *num_pairs = h[1];
+  if (capacity_needed) *capacity_needed = h[4];
+  if (tile_pairs) *tile_pairs = h[1];
   return (h[0] & kFlagPairOverflow) ? DSPLAT_ERR_CAPACITY : DSPLAT_OK;
 }
 

@@ -12,7 +12,10 @@
 // A warp stages 32 list entries at a time into its own shared-memory slots
 // (one coalesced index load + one 48-byte record gather per lane), then every
 // lane walks them with 128-bit broadcast reads, amortising each read over its
-// pixels.  The warp stops fetching as soon as all its pixels terminated
+// pixels.  The fused path reads each tile's entries straight out of its
+// superblock list (8x8 tiles, see tiles.cu): a ballot over the 32 fetched
+// entries keeps those whose tile span covers the tile, compacted in order, so
+// no per-tile list is ever materialised.  The warp stops fetching as soon as all its pixels terminated
 // (__any_sync), so no CTA-wide barrier exists anywhere.  Warps pull tasks
 // from a global counter (work stealing): one persistent launch covers views
 // of different resolutions.
@@ -76,6 +79,45 @@ struct PackedSrc {
   __device__ __forceinline__ void stage(Ent* dst, uint32_t g) const { stage_packed(dst, rec, g); }
 };
 
+// Entry walkers: stage up to 32 entries of the list position range
+// [pos0 - 32, pos0) (backwards) or [pos0, pos0 + 32) (forwards) into the
+// warp's slots, in walk order, with each entry's list position in d.z;
+// return how many were staged.
+struct TileWalk {  // a per-tile list (tile2idx / idx2pnt)
+  const uint32_t* idx2pnt;
+  template <class Src>
+  __device__ __forceinline__ int stage(const Src& src, Ent* sm, uint32_t pos, bool valid, int lane) const {
+    if (valid) {
+      src.stage(&sm[lane], idx2pnt[pos]);
+      sm[lane].d.z = __uint_as_float(pos);
+    }
+    return __popc(__ballot_sync(0xffffffffu, valid));
+  }
+};
+
+struct SbWalk {  // a superblock list filtered to one tile (ballot compaction keeps the order)
+  const uint2* list1;
+  uint32_t lx, ly;  // tile position inside its superblock
+  template <class Src>
+  __device__ __forceinline__ int stage(const Src& src, Ent* sm, uint32_t pos, bool valid, int lane) const {
+    bool m = false;
+    uint32_t g = 0;
+    if (valid) {
+      const uint2 en = list1[pos];
+      g = en.x;
+      const uint32_t lr = en.y;
+      m = lx >= (lr & 15u) && lx < ((lr >> 8) & 15u) && ly >= ((lr >> 4) & 15u) && ly < (lr >> 12);
+    }
+    const uint32_t bal = __ballot_sync(0xffffffffu, m);
+    if (m) {
+      const int slot = __popc(bal & ((1u << lane) - 1u));
+      src.stage(&sm[slot], g);
+      sm[slot].d.z = __uint_as_float(pos);
+    }
+    return __popc(bal);
+  }
+};
+
 // q = d^T K d exactly as the reference's mult_vec_from_both_sides orders it:
 // (A dx) dx + B (dx dy + dy dx) + (C dy) dy
 __device__ __forceinline__ float quad(float B, float C, float dx, float dy, float adxdx) {
@@ -84,14 +126,19 @@ __device__ __forceinline__ float quad(float B, float C, float dx, float dy, floa
 }
 
 // ---------------------------------------------------------------------------
-// Forward walk of one slab by one warp.
+// Forward walk of one slab by one warp over the list range [s, e).
+// Every pixel slot of a lane is evaluated branch-free: a slot that is done or
+// outside the entry's box gets alpha = 0, which leaves colour, T and
+// alpha_sum bit-for-bit unchanged (x*0 = +-0 and y + +-0 = y), so the result
+// equals the reference's skip-and-break walk while the 8 slots run in
+// parallel (instruction-level parallelism).
 // ---------------------------------------------------------------------------
-template <int TS, class Src>
-__device__ __forceinline__ void fwd_slab(const Src& src, Ent* sm, const uint32_t* __restrict__ idx2pnt, uint32_t s,
-                                         uint32_t e, int px0, int py0, int w, int h, bool accumulate,
-                                         float* __restrict__ out_rgb, size_t pix_base, float* __restrict__ out_T,
-                                         uint32_t* __restrict__ out_last, const float* __restrict__ target,
-                                         float* __restrict__ grad_pix, float* __restrict__ loss_slot) {
+template <int TS, class Walk, class Src>
+__device__ __forceinline__ void fwd_slab(const Walk& walk, const Src& src, Ent* sm, uint32_t s, uint32_t e, int px0,
+                                         int py0, int w, int h, bool accumulate, float* __restrict__ out_rgb,
+                                         size_t pix_base, float* __restrict__ out_T, uint32_t* __restrict__ out_last,
+                                         const float* __restrict__ target, float* __restrict__ grad_pix,
+                                         float* __restrict__ loss_slot) {
   using G = Geo<TS>;
   constexpr int PPL = G::PPL;
   const int lane = threadIdx.x & 31;
@@ -121,31 +168,36 @@ __device__ __forceinline__ void fwd_slab(const Src& src, Ent* sm, const uint32_t
   const uint32_t inside = live;
   for (uint32_t hi = e; hi > s;) {
     const int cnt = int(min(32u, hi - s));
-    if (lane < cnt) src.stage(&sm[lane], idx2pnt[hi - 1u - uint32_t(lane)]);
+    const int k_staged = walk.stage(src, sm, hi - 1u - uint32_t(lane), lane < cnt, lane);
     __syncwarp();
     if (live) {
-      for (int j = 0; j < cnt; ++j) {
+      for (int j = 0; j < k_staged; ++j) {
         const float4 ea = sm[j].a, eb = sm[j].b, ec = sm[j].c, ed = sm[j].d;
         if (!(ec.y <= fx && fx <= ec.w)) continue;
         const float dx = fs(fx, ea.x);
         const float adxdx = fm(fm(ea.z, dx), dx);
+        float al[PPL];
 #pragma unroll
         for (int k = 0; k < PPL; ++k) {
-          if (!((live >> k) & 1u)) continue;
           const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
-          if (!(ec.z <= fy && fy <= ed.x)) continue;
+          const bool act = ((live >> k) & 1u) && ec.z <= fy && fy <= ed.x;
           const float dy = fs(fy, ea.y);
           const float q = quad(ea.w, eb.x, dx, dy, adxdx);
-          const float al = fm(dexp(fm(-0.5f, q)), eb.y);
-          const float eo = fm(T[k], al);
+          const float a = fm(dexp(fm(-0.5f, q)), eb.y);
+          al[k] = act ? a : 0.f;
+        }
+        const uint32_t pos = __float_as_uint(ed.z);
+#pragma unroll
+        for (int k = 0; k < PPL; ++k) {
+          const float eo = fm(T[k], al[k]);
           c0[k] = fa(c0[k], fm(eb.z, eo));
           c1[k] = fa(c1[k], fm(eb.w, eo));
           c2[k] = fa(c2[k], fm(ec.x, eo));
-          T[k] = fm(T[k], fs(1.f, al));
+          T[k] = fm(T[k], fs(1.f, al[k]));
           as[k] = fa(as[k], eo);
-          if (as[k] >= kAlphaBreak) {
+          if (((live >> k) & 1u) && as[k] >= kAlphaBreak) {
             live &= ~(1u << k);
-            last[k] = hi - 1u - uint32_t(j);
+            last[k] = pos;
           }
         }
         if (!live) break;
@@ -181,16 +233,41 @@ __device__ __forceinline__ void fwd_slab(const Src& src, Ent* sm, const uint32_t
   }
 }
 
+// The superblock-list range of an item and the tile's place in it.
+struct ItemGeo {
+  int v, px0, py0;
+  uint32_t s, e, lx, ly;
+};
+
+__device__ __forceinline__ ItemGeo item_geo(const ViewBatch& b, uint32_t item, const uint32_t* __restrict__ off1,
+                                            uint32_t nchunk, uint64_t capacity) {
+  ItemGeo g;
+  g.v = view_of_item(b, item);
+  const ViewDev& vd = b.v[g.v];
+  const uint32_t t = item - vd.item_base;
+  const uint32_t tx = t % uint32_t(vd.tile_w), ty = t / uint32_t(vd.tile_w);
+  const uint32_t sbw = uint32_t(vd.tile_w + 7) >> 3;
+  const uint32_t sb = vd.sb_base + (ty >> 3) * sbw + (tx >> 3);
+  g.s = uint32_t(min(uint64_t(off1[size_t(sb) * nchunk]), capacity));
+  g.e = uint32_t(min(uint64_t(off1[size_t(sb + 1) * nchunk]), capacity));
+  g.lx = tx & 7u;
+  g.ly = ty & 7u;
+  g.px0 = int(tx) * b.ts;
+  g.py0 = int(ty) * b.ts;
+  return g;
+}
+
 // ---------------------------------------------------------------------------
-// Fused-path forward: persistent, per-warp work stealing over slab tasks.
+// Fused-path forward: persistent, per-warp work stealing over slab tasks,
+// walking each tile's entries out of its superblock list.
 // slab_loss: one partial L2 loss per task (when target is given).
 // ---------------------------------------------------------------------------
 template <int TS>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
-    const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint32_t* __restrict__ item_start,
-    const uint32_t* __restrict__ idx2pnt, uint32_t* __restrict__ work_counter, float* __restrict__ out_rgb,
-    float* __restrict__ out_T, uint32_t* __restrict__ out_last, const float* __restrict__ target,
-    float* __restrict__ grad_pix, float* __restrict__ slab_loss) {
+    const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint2* __restrict__ list1,
+    const uint32_t* __restrict__ off1, uint32_t nchunk, uint64_t capacity, uint32_t* __restrict__ work_counter,
+    float* __restrict__ out_rgb, float* __restrict__ out_T, uint32_t* __restrict__ out_last,
+    const float* __restrict__ target, float* __restrict__ grad_pix, float* __restrict__ slab_loss) {
   using G = Geo<TS>;
   __shared__ Ent sm_all[kRasterWarps][32];
   Ent* sm = sm_all[threadIdx.x >> 5];
@@ -202,19 +279,18 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     task = __shfl_sync(0xffffffffu, task, 0);
     if (task >= num_tasks) return;
     const uint32_t item = task / G::SLABS, slab = task % G::SLABS;
-    const int v = view_of_item(b, item);
-    const ViewDev& vd = b.v[v];
-    const uint32_t t = item - vd.item_base;
-    const int px0 = int(t % uint32_t(vd.tile_w)) * TS;
-    const int py0 = int(t / uint32_t(vd.tile_w)) * TS + int(slab) * G::SLAB_ROWS;
-    PackedSrc src{rec + 3 * size_t(v) * n};
-    fwd_slab<TS>(src, sm, idx2pnt, item_start[item], item_start[item + 1], px0, py0, vd.w, vd.h, false, out_rgb,
+    const ItemGeo ig = item_geo(b, item, off1, nchunk, capacity);
+    const ViewDev& vd = b.v[ig.v];
+    PackedSrc src{rec + 3 * size_t(ig.v) * n};
+    SbWalk walk{list1, ig.lx, ig.ly};
+    fwd_slab<TS>(walk, src, sm, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, false, out_rgb,
                  vd.pix_base, out_T, out_last, target, grad_pix, slab_loss ? slab_loss + task : nullptr);
     __syncwarp();
   }
 }
 
-// Drop-in forward (splat_gauss.rs:46-94): AoS inputs, accumulates into pix2rgb.
+// Drop-in forward (splat_gauss.rs:46-94): AoS inputs and per-tile lists,
+// accumulates into pix2rgb.
 template <int TS>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
     int w, int h, int tile_w, uint32_t num_tasks, float* __restrict__ pix2rgb, AosSrc src,
@@ -228,19 +304,25 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
   const uint32_t tile = task / G::SLABS, slab = task % G::SLABS;
   const int px0 = int(tile % uint32_t(tile_w)) * TS;
   const int py0 = int(tile / uint32_t(tile_w)) * TS + int(slab) * G::SLAB_ROWS;
-  fwd_slab<TS>(src, sm, idx2pnt, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, true, pix2rgb, 0, out_T,
-               out_last, nullptr, nullptr, nullptr);
+  TileWalk walk{idx2pnt};
+  fwd_slab<TS>(walk, src, sm, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, true, pix2rgb, 0, out_T, out_last,
+               nullptr, nullptr, nullptr);
 }
 
 // ---------------------------------------------------------------------------
 // Fused-path backward.  grad2d[(v*N+g)*3 + k] float4:
 //   (d px, d py, d A, d B) (d C, d opacity, d r, d g) (d b, 0, 0, 0)
+// Inactive slots get G = 0, which makes every update below a no-op, so the
+// 8 slots are evaluated branch-free.  exp and 1/(1-alpha) use the hardware
+// approximations: gradients need not reproduce the forward bit for bit (the
+// discrete structure -- boxes, stop positions -- comes from the forward).
 // ---------------------------------------------------------------------------
 template <int TS>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
-    const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint32_t* __restrict__ item_start,
-    const uint32_t* __restrict__ idx2pnt, uint32_t* __restrict__ work_counter, const float* __restrict__ grad_pix,
-    const float* __restrict__ pix_T, const uint32_t* __restrict__ pix_last, float4* __restrict__ grad2d) {
+    const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint2* __restrict__ list1,
+    const uint32_t* __restrict__ off1, uint32_t nchunk, uint64_t capacity, uint32_t* __restrict__ work_counter,
+    const float* __restrict__ grad_pix, const float* __restrict__ pix_T, const uint32_t* __restrict__ pix_last,
+    float4* __restrict__ grad2d) {
   using G = Geo<TS>;
   constexpr int PPL = G::PPL;
   __shared__ Ent sm_all[kRasterWarps][32];
@@ -253,13 +335,12 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     task = __shfl_sync(0xffffffffu, task, 0);
     if (task >= num_tasks) return;
     const uint32_t item = task / G::SLABS, slab = task % G::SLABS;
-    const int v = view_of_item(b, item);
-    const ViewDev& vd = b.v[v];
-    const uint32_t t = item - vd.item_base;
-    const int ix = int(t % uint32_t(vd.tile_w)) * TS + (lane % TS);
-    const int iy0 = int(t / uint32_t(vd.tile_w)) * TS + int(slab) * G::SLAB_ROWS + (lane / TS);
+    const ItemGeo ig = item_geo(b, item, off1, nchunk, capacity);
+    const ViewDev& vd = b.v[ig.v];
+    const int ix = ig.px0 + (lane % TS);
+    const int iy0 = ig.py0 + int(slab) * G::SLAB_ROWS + (lane / TS);
     const float fx = float(ix) + 0.5f;
-    const uint32_t s = item_start[item], e = item_start[item + 1];
+    const uint32_t s = ig.s, e = ig.e;
     float Tc[PPL], a0[PPL], a1[PPL], a2[PPL], d0[PPL], d1[PPL], d2[PPL];
     uint32_t last[PPL];
     uint32_t lo_min = e;
@@ -282,15 +363,16 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lo_min = min(lo_min, __shfl_xor_sync(0xffffffffu, lo_min, o));
-    const float4* recv = rec + 3 * size_t(v) * n;
-    float4* gv = grad2d + 3 * size_t(v) * n;
+    PackedSrc src{rec + 3 * size_t(ig.v) * n};
+    SbWalk walk{list1, ig.lx, ig.ly};
+    float4* gv = grad2d + 3 * size_t(ig.v) * n;
     for (uint32_t lo = max(s, lo_min); lo < e; lo += 32) {
       const int cnt = int(min(32u, e - lo));
-      if (lane < cnt) stage_packed(&sm[lane], recv, idx2pnt[lo + uint32_t(lane)]);
+      const int k_staged = walk.stage(src, sm, lo + uint32_t(lane), lane < cnt, lane);
       __syncwarp();
-      for (int j = 0; j < cnt; ++j) {
+      for (int j = 0; j < k_staged; ++j) {
         const float4 ea = sm[j].a, eb = sm[j].b, ec = sm[j].c, ed = sm[j].d;
-        const uint32_t pos = lo + uint32_t(j);
+        const uint32_t pos = __float_as_uint(ed.z);
         float gpx = 0.f, gpy = 0.f, gA = 0.f, gB = 0.f, gC = 0.f, gop = 0.f, gr = 0.f, gg = 0.f, gb = 0.f;
         bool any = false;
         if (ec.y <= fx && fx <= ec.w) {
@@ -300,14 +382,13 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
 #pragma unroll
           for (int k = 0; k < PPL; ++k) {
             const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
-            if (pos < last[k] || !(ec.z <= fy && fy <= ed.x)) continue;
-            any = true;
+            const bool act = pos >= last[k] && ec.z <= fy && fy <= ed.x;
+            any |= act;
             const float dy = fs(fy, ea.y);
             const float q = quad(B, C, dx, dy, adxdx);
-            const float Gv = dexp(fm(-0.5f, q));
-            const float al = fm(Gv, op);
-            const float om = 1.f - al;
-            const float iom = 1.f / om;
+            const float Gv = act ? __expf(-0.5f * q) : 0.f;
+            const float al = Gv * op;
+            const float iom = __frcp_rn(1.f - al);
             Tc[k] = Tc[k] * iom;
             const float wgt = al * Tc[k];
             const float dLde = d0[k] * (eb.z * Tc[k] - a0[k] * iom) + d1[k] * (eb.w * Tc[k] - a1[k] * iom) +
@@ -427,25 +508,25 @@ static int persistent_grid(K kernel, uint32_t tasks) {
 }
 
 template <int TS>
-static void launch_fwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint32_t* item_start,
-                       const uint32_t* idx2pnt, uint32_t* counter, float* out_rgb, float* out_T, uint32_t* out_last,
-                       const float* target, float* grad_pix, float* slab_loss) {
-  static int grid_per_task = 0;  // cached occupancy-derived grid
+static void launch_fwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint2* list1,
+                       const uint32_t* off1, uint32_t nchunk, uint64_t capacity, uint32_t* counter, float* out_rgb,
+                       float* out_T, uint32_t* out_last, const float* target, float* grad_pix, float* slab_loss) {
+  static int grid = 0;
   static uint32_t cached_tasks = 0;
   const uint32_t tasks = b.num_items * Geo<TS>::SLABS;
-  if (!grid_per_task || cached_tasks != tasks) {
-    grid_per_task = persistent_grid(k_raster_fwd<TS>, tasks);
+  if (!grid || cached_tasks != tasks) {
+    grid = persistent_grid(k_raster_fwd<TS>, tasks);
     cached_tasks = tasks;
   }
-  k_raster_fwd<TS><<<grid_per_task, 32 * kRasterWarps, 0, st>>>(b, n, rec, item_start, idx2pnt, counter, out_rgb,
-                                                                out_T, out_last, target, grad_pix, slab_loss);
+  k_raster_fwd<TS><<<grid, 32 * kRasterWarps, 0, st>>>(b, n, rec, list1, off1, nchunk, capacity, counter, out_rgb,
+                                                       out_T, out_last, target, grad_pix, slab_loss);
   count_launch();
 }
 
 template <int TS>
-static void launch_bwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint32_t* item_start,
-                       const uint32_t* idx2pnt, uint32_t* counter, const float* grad_pix, const float* pix_T,
-                       const uint32_t* pix_last, float4* grad2d) {
+static void launch_bwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint2* list1,
+                       const uint32_t* off1, uint32_t nchunk, uint64_t capacity, uint32_t* counter,
+                       const float* grad_pix, const float* pix_T, const uint32_t* pix_last, float4* grad2d) {
   static int grid = 0;
   static uint32_t cached_tasks = 0;
   const uint32_t tasks = b.num_items * Geo<TS>::SLABS;
@@ -453,25 +534,26 @@ static void launch_bwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const fl
     grid = persistent_grid(k_raster_bwd<TS>, tasks);
     cached_tasks = tasks;
   }
-  k_raster_bwd<TS><<<grid, 32 * kRasterWarps, 0, st>>>(b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T,
-                                                       pix_last, grad2d);
+  k_raster_bwd<TS><<<grid, 32 * kRasterWarps, 0, st>>>(b, n, rec, list1, off1, nchunk, capacity, counter, grad_pix,
+                                                       pix_T, pix_last, grad2d);
   count_launch();
 }
 
-cudaError_t raster_fwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint32_t* item_start,
-                       const uint32_t* idx2pnt, uint32_t* counter, float* out_rgb, float* out_T, uint32_t* out_last,
-                       const float* target, float* grad_pix, float* slab_loss) {
+cudaError_t raster_fwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint2* list1,
+                       const uint32_t* off1, uint32_t nchunk, uint64_t capacity, uint32_t* counter, float* out_rgb,
+                       float* out_T, uint32_t* out_last, const float* target, float* grad_pix, float* slab_loss) {
   switch (b.ts) {
     case 8:
-      launch_fwd<8>(st, b, n, rec, item_start, idx2pnt, counter, out_rgb, out_T, out_last, target, grad_pix, slab_loss);
+      launch_fwd<8>(st, b, n, rec, list1, off1, nchunk, capacity, counter, out_rgb, out_T, out_last, target, grad_pix,
+                    slab_loss);
       break;
     case 16:
-      launch_fwd<16>(st, b, n, rec, item_start, idx2pnt, counter, out_rgb, out_T, out_last, target, grad_pix,
-                     slab_loss);
+      launch_fwd<16>(st, b, n, rec, list1, off1, nchunk, capacity, counter, out_rgb, out_T, out_last, target,
+                     grad_pix, slab_loss);
       break;
     case 32:
-      launch_fwd<32>(st, b, n, rec, item_start, idx2pnt, counter, out_rgb, out_T, out_last, target, grad_pix,
-                     slab_loss);
+      launch_fwd<32>(st, b, n, rec, list1, off1, nchunk, capacity, counter, out_rgb, out_T, out_last, target,
+                     grad_pix, slab_loss);
       break;
     default:
       return cudaErrorInvalidValue;
@@ -479,18 +561,18 @@ cudaError_t raster_fwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const fl
   return cudaGetLastError();
 }
 
-cudaError_t raster_bwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint32_t* item_start,
-                       const uint32_t* idx2pnt, uint32_t* counter, const float* grad_pix, const float* pix_T,
-                       const uint32_t* pix_last, float4* grad2d) {
+cudaError_t raster_bwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint2* list1,
+                       const uint32_t* off1, uint32_t nchunk, uint64_t capacity, uint32_t* counter,
+                       const float* grad_pix, const float* pix_T, const uint32_t* pix_last, float4* grad2d) {
   switch (b.ts) {
     case 8:
-      launch_bwd<8>(st, b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T, pix_last, grad2d);
+      launch_bwd<8>(st, b, n, rec, list1, off1, nchunk, capacity, counter, grad_pix, pix_T, pix_last, grad2d);
       break;
     case 16:
-      launch_bwd<16>(st, b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T, pix_last, grad2d);
+      launch_bwd<16>(st, b, n, rec, list1, off1, nchunk, capacity, counter, grad_pix, pix_T, pix_last, grad2d);
       break;
     case 32:
-      launch_bwd<32>(st, b, n, rec, item_start, idx2pnt, counter, grad_pix, pix_T, pix_last, grad2d);
+      launch_bwd<32>(st, b, n, rec, list1, off1, nchunk, capacity, counter, grad_pix, pix_T, pix_last, grad2d);
       break;
     default:
       return cudaErrorInvalidValue;

@@ -278,6 +278,15 @@ __device__ __forceinline__ bool sb_span(uint2 rc, int* sx0, int* sy0, int* sx1, 
   return true;
 }
 
+// tile span clipped to superblock (sx, sy), in local tile coordinates 0..8:
+// x0 | y0 << 4 | x1 << 8 | y1 << 12
+__device__ __forceinline__ uint32_t local_rect(uint2 rc, int sx, int sy) {
+  const int bx = sx * 8, by = sy * 8;
+  const int x0 = max(int(rc.x & 0xffff), bx) - bx, x1 = min(int(rc.y & 0xffff), bx + 8) - bx;
+  const int y0 = max(int(rc.x >> 16), by) - by, y1 = min(int(rc.y >> 16), by + 8) - by;
+  return uint32_t(x0) | uint32_t(y0) << 4 | uint32_t(x1) << 8 | uint32_t(y1) << 12;
+}
+
 constexpr int kMsThreads = 256;
 constexpr int kMsWarps = kMsThreads / 32;
 constexpr int kMsRounds = 16;
@@ -346,7 +355,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
                                                            const uint2* __restrict__ rect, uint32_t n, uint32_t npad,
                                                            const ViewBatch b,
                                                            const uint32_t* __restrict__ off, uint64_t capacity,
-                                                           uint32_t* __restrict__ list1, uint32_t* __restrict__ flags) {
+                                                           uint2* __restrict__ list1, uint32_t* __restrict__ flags) {
   extern __shared__ uint32_t wc[];  // [kMsWarps][nsb]
   const uint32_t nchunk = npad / kMsChunk;
   const uint32_t v = blockIdx.x / nchunk, c = blockIdx.x % nchunk;
@@ -383,7 +392,8 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
   for (int r = 0; r < kMsRounds; ++r) {
     const uint32_t g = order[base + r * 32 + lane];
     int sx0 = 0, sy0 = 0, sx1 = 0, sy1 = 0;
-    const bool has = g < n && sb_span(rect[size_t(v) * n + g], &sx0, &sy0, &sx1, &sy1);
+    const uint2 rc = g < n ? rect[size_t(v) * n + g] : make_uint2(0u, 0u);
+    const bool has = g < n && sb_span(rc, &sx0, &sy0, &sx1, &sy1);
     const uint32_t packed =
         has ? (uint32_t(sx0) | uint32_t(sy0) << 8 | uint32_t(sx1) << 16 | uint32_t(sy1) << 24) : 0u;
 #pragma unroll
@@ -393,7 +403,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
         int below, above;
         lane_rank(spans, lane, sx, sy, &below, &above);
         const uint32_t dst = my[sy * sbw + sx] + uint32_t(below);
-        if (dst < capacity) list1[dst] = g;
+        if (dst < capacity) list1[dst] = make_uint2(g, local_rect(rc, sx, sy));
         else set_flag(flags, kFlagPairOverflow);
       }
     __syncwarp();
@@ -418,10 +428,9 @@ __device__ __forceinline__ int view_of_sb(const ViewBatch& b, uint32_t sb) {
   return v;
 }
 
-__global__ void __launch_bounds__(kMsThreads) k_tile_count(const uint32_t* __restrict__ list1,
+__global__ void __launch_bounds__(kMsThreads) k_tile_count(const uint2* __restrict__ list1,
                                                            const uint32_t* __restrict__ off1, uint32_t nchunk,
-                                                           uint64_t capacity, const uint2* __restrict__ rect,
-                                                           uint32_t n, const ViewBatch b,
+                                                           uint64_t capacity, const ViewBatch b,
                                                            uint32_t* __restrict__ tcnt) {
   __shared__ uint32_t h[64];
   const uint32_t sb = blockIdx.x;
@@ -435,11 +444,10 @@ __global__ void __launch_bounds__(kMsThreads) k_tile_count(const uint32_t* __res
   const uint64_t s = min(uint64_t(off1[size_t(sb) * nchunk]), capacity);
   const uint64_t e = min(uint64_t(off1[size_t(sb + 1) * nchunk]), capacity);
   for (uint64_t i = s + threadIdx.x; i < e; i += kMsThreads) {
-    const uint2 rc = rect[size_t(v) * n + list1[i]];
-    const int x0 = max(int(rc.x & 0xffff), tx0), x1 = min(int(rc.y & 0xffff), tx0 + 8);
-    const int y0 = max(int(rc.x >> 16), ty0), y1 = min(int(rc.y >> 16), ty0 + 8);
+    const uint32_t lr = list1[i].y;
+    const int x0 = lr & 15, y0 = (lr >> 4) & 15, x1 = (lr >> 8) & 15, y1 = (lr >> 12) & 15;
     for (int y = y0; y < y1; ++y)
-      for (int x = x0; x < x1; ++x) atomicAdd(&h[(y - ty0) * 8 + (x - tx0)], 1u);
+      for (int x = x0; x < x1; ++x) atomicAdd(&h[y * 8 + x], 1u);
   }
   __syncthreads();
   if (threadIdx.x < 64) {
@@ -455,10 +463,9 @@ __global__ void __launch_bounds__(kMsThreads) k_tile_count(const uint32_t* __res
 //   slot = tile start + earlier chunks + earlier warps + lower lanes.
 // out_tile (nullable) receives each pair's item id.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kMsThreads) k_tile_scatter(const uint32_t* __restrict__ list1,
+__global__ void __launch_bounds__(kMsThreads) k_tile_scatter(const uint2* __restrict__ list1,
                                                              const uint32_t* __restrict__ off1, uint32_t nchunk,
-                                                             uint64_t capacity, const uint2* __restrict__ rect,
-                                                             uint32_t n, const ViewBatch b,
+                                                             uint64_t capacity, const ViewBatch b,
                                                                const uint32_t* __restrict__ item_start,
                                                              uint32_t* __restrict__ idx2pnt,
                                                              uint32_t* __restrict__ out_tile,
@@ -487,12 +494,12 @@ __global__ void __launch_bounds__(kMsThreads) k_tile_scatter(const uint32_t* __r
     uint32_t g = 0;
     int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
     if (i < e) {
-      g = list1[i];
-      const uint2 rc = rect[size_t(v) * n + g];
-      x0 = max(int(rc.x & 0xffff), tx0) - tx0;
-      x1 = min(int(rc.y & 0xffff), tx0 + 8) - tx0;
-      y0 = max(int(rc.x >> 16), ty0) - ty0;
-      y1 = min(int(rc.y >> 16), ty0 + 8) - ty0;
+      const uint2 en = list1[i];
+      g = en.x;
+      x0 = en.y & 15;
+      y0 = (en.y >> 4) & 15;
+      x1 = (en.y >> 8) & 15;
+      y1 = (en.y >> 12) & 15;
     }
 #pragma unroll
     for (int k = 0; k < 64; ++k) {

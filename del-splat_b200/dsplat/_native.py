@@ -50,11 +50,11 @@ class GaussGrads(ctypes.Structure):
 
 class BatchLayout(ctypes.Structure):
     _fields_ = [("total_bytes", c_size), ("num_items", c_u32), ("num_pix", c_u32), ("npad", c_u32),
-                ("slabs_per_tile", c_u32),
+                ("slabs_per_tile", c_u32), ("num_sb", c_u32), ("sb_chunks", c_u32),
                 ("off_flags", c_size), ("off_rec", c_size), ("off_rect", c_size), ("off_cnt", c_size),
-                ("off_order", c_size), ("off_item_start", c_size), ("off_idx2pnt", c_size),
-                ("off_sb_list", c_size), ("off_pix_T", c_size), ("off_pix_stop", c_size),
-                ("off_grad_pix", c_size), ("off_slab_loss", c_size), ("off_grad2d", c_size)]
+                ("off_order", c_size), ("off_sb_start", c_size), ("off_sb_list", c_size),
+                ("off_pix_T", c_size), ("off_pix_stop", c_size), ("off_grad_pix", c_size),
+                ("off_slab_loss", c_size), ("off_grad2d", c_size)]
 
 
 _P = c_void_p  # every pointer is passed as an integer address
@@ -82,7 +82,8 @@ SIGNATURES = {
                                            c_u64, _P, c_size, _P, _P, _P]),
     "dsplat_gauss_batch_backward": (c_i32, [_P, ctypes.POINTER(GaussParams), c_i32, ctypes.POINTER(View), c_i32,
                                             c_u64, _P, c_size, _P, ctypes.POINTER(GaussGrads)]),
-    "dsplat_gauss_batch_status": (c_i32, [_P, _P, ctypes.POINTER(c_u32), ctypes.POINTER(c_u64)]),
+    "dsplat_gauss_batch_status": (c_i32, [_P, _P, ctypes.POINTER(c_u32), ctypes.POINTER(c_u64),
+                                          ctypes.POINTER(c_u64)]),
     "dsplat_set_stage_events": (c_i32, [ctypes.POINTER(c_void_p), c_i32]),
     "dsplat_adam_step": (c_i32, [_P, c_i64, _P, _P, _P, _P, c_f32, c_f32, c_f32, c_f32, c_i32]),
 }

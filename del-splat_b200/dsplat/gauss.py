@@ -81,23 +81,25 @@ class GaussBatch:
         self.out_rgb = torch.empty(int(L.num_pix) * 3, dtype=torch.float32, device=self.device)
 
     def ensure_capacity(self, params: Dict[str, torch.Tensor], slack: float = 1.05) -> int:
-        """Run one forward, read the pair total and grow the pair buffers."""
+        """Run one forward, read the capacity it needed and grow the lists; returns the tile pairs."""
         self.forward(params)
-        flags, pairs = self.status()
-        if pairs > self.capacity:
-            self._alloc(int(pairs * slack) + 1024)
+        flags, needed, pairs = self.status()
+        if needed > self.capacity:
+            self._alloc(int(needed * slack) + 1024)
             self.forward(params)
-            flags, pairs = self.status()
+            flags, needed, pairs = self.status()
             if flags:
-                raise RuntimeError("pair capacity still exceeded after resize")
+                raise RuntimeError("list capacity still exceeded after resize")
         return pairs
 
     def status(self):
+        """(flags, capacity needed, tile pairs) of the last forward (synchronises)."""
         f = N.c_u32(0)
+        need = N.c_u64(0)
         p = N.c_u64(0)
         N.lib().dsplat_gauss_batch_status(_stream_ptr(self.device), self.ws.data_ptr(), ctypes.byref(f),
-                                          ctypes.byref(p))
-        return int(f.value), int(p.value)
+                                          ctypes.byref(need), ctypes.byref(p))
+        return int(f.value), int(need.value), int(p.value)
 
     # ----------------------------------------------------------- launches
     def forward(self, params: Dict[str, torch.Tensor], target: Optional[torch.Tensor] = None,
@@ -149,20 +151,41 @@ class GaussBatch:
                 for v, c in enumerate(self.cameras)]
 
     def tile_lists(self, view: int):
-        """(tile2idx [T+1], idx2pnt [P_v]) of one view, in the reference's format."""
+        """Per-tile lists of one view in the reference's format, rebuilt on the host
+        from the superblock lists: (tile2idx [T+1] u32, idx2pnt [P] u32,
+        stop [H,W] i64 = each pixel's stop position as an idx2pnt position)."""
         L = self.layout
         ts = self.tile_size
-        item_base = 0
-        for v in range(view):
-            c = self.cameras[v]
-            item_base += ((c.width + ts - 1) // ts) * ((c.height + ts - 1) // ts)
+        sb_base = 0
+        for c in self.cameras[:view]:
+            tw_, th_ = (c.width + ts - 1) // ts, (c.height + ts - 1) // ts
+            sb_base += ((tw_ + 7) // 8) * ((th_ + 7) // 8)
         c = self.cameras[view]
-        T = ((c.width + ts - 1) // ts) * ((c.height + ts - 1) // ts)
-        starts = self._ws(L.off_item_start, int(L.num_items) + 1, torch.int32)
-        s = starts[item_base: item_base + T + 1].to(torch.int64)
-        idx = self._ws(L.off_idx2pnt, self.capacity, torch.int32)
-        p0, p1 = int(s[0]), int(s[-1])
-        return (s - p0).to(torch.int32), idx[p0:p1]
+        tw, th = (c.width + ts - 1) // ts, (c.height + ts - 1) // ts
+        sbw = (tw + 7) // 8
+        ch = int(L.sb_chunks)
+        starts = self._ws(L.off_sb_start, int(L.num_sb) * ch + 1, torch.int32).cpu().numpy().view(np.uint32)
+        ent = self._ws(L.off_sb_list, 2 * self.capacity, torch.int32).cpu().numpy().view(np.uint32).reshape(-1, 2)
+        stop_sb = self.per_pixel("stop")[view].cpu().numpy().view(np.uint32).astype(np.int64)
+        tile2idx = np.zeros(tw * th + 1, np.uint32)
+        lists, positions = [], []
+        for t in range(tw * th):
+            tx, ty = t % tw, t // tw
+            sb = sb_base + (ty // 8) * sbw + (tx // 8)
+            s, e = int(starts[sb * ch]), int(starts[(sb + 1) * ch])
+            lr = ent[s:e, 1]
+            lx, ly = tx % 8, ty % 8
+            m = (lx >= (lr & 15)) & (lx < ((lr >> 8) & 15)) & (ly >= ((lr >> 4) & 15)) & (ly < (lr >> 12))
+            lists.append(ent[s:e, 0][m])
+            positions.append(s + np.nonzero(m)[0])
+            tile2idx[t + 1] = tile2idx[t] + int(m.sum())
+        idx2pnt = np.concatenate(lists).astype(np.uint32) if lists else np.zeros(0, np.uint32)
+        stop = np.zeros((c.height, c.width), np.int64)
+        for t in range(tw * th):
+            tx, ty = t % tw, t // tw
+            ys, xs = slice(ty * ts, min(ty * ts + ts, c.height)), slice(tx * ts, min(tx * ts + ts, c.width))
+            stop[ys, xs] = tile2idx[t] + np.searchsorted(positions[t], stop_sb[ys, xs])
+        return tile2idx, idx2pnt, stop
 
     def slab_loss(self) -> torch.Tensor:
         """Partial L2 losses of the last forward with a target (sum = loss)."""

@@ -158,23 +158,31 @@ typedef struct { /* gradients, accumulated (+=) */
   float* colors;
 } dsplat_gauss_grads;
 
-/* Byte offsets of the batch state inside the workspace (for inspection). */
+/* Byte offsets of the batch state inside the workspace (for inspection).
+ * Tile lists of the batched path live in superblock form: superblock s
+ * (8x8 tiles; view v's superblocks start at the sum of the earlier views'
+ * counts, row-major inside the view) owns the entries
+ * sb_list[sb_start[s * sb_chunks] .. sb_start[(s + 1) * sb_chunks]), each a
+ * (point index, span) pair where span packs the tiles it covers inside the
+ * superblock as x0 | y0 << 4 | x1 << 8 | y1 << 12; filtering a superblock list
+ * by tile gives that tile's list in the reference's order. */
 typedef struct {
   size_t total_bytes;
   uint32_t num_items; /* sum over views of tiles */
   uint32_t num_pix;   /* sum over views of pixels */
   uint32_t npad;      /* per-view padded point count of the depth sort */
   uint32_t slabs_per_tile; /* raster warp tasks per tile (4 for 32x32 tiles, else 1) */
-  size_t off_flags;      /* u32[4]: flags, total pairs, counters */
+  uint32_t num_sb;    /* superblocks over all views */
+  uint32_t sb_chunks; /* entries of sb_start per superblock */
+  size_t off_flags;      /* u32[16]: [0] flags, [1] tile pairs, [4] superblock entries */
   size_t off_rec;        /* float4[V*N*3] per-view 2D records */
   size_t off_rect;       /* uint2[V*N] tile spans */
   size_t off_cnt;        /* u32[V*N] tiles per point */
   size_t off_order;      /* u32[V*npad] points in depth order per view */
-  size_t off_item_start; /* u32[num_items+1] */
-  size_t off_idx2pnt;    /* u32[capacity] points sorted by (item, depth) */
-  size_t off_sb_list;    /* u32[capacity] stage-1 superblock lists */
+  size_t off_sb_start;   /* u32[num_sb*sb_chunks+1] superblock list offsets */
+  size_t off_sb_list;    /* uint2[capacity] superblock lists */
   size_t off_pix_T;      /* f32[num_pix] final transmittance */
-  size_t off_pix_stop;   /* u32[num_pix] list position where the walk stopped */
+  size_t off_pix_stop;   /* u32[num_pix] sb_list position where the walk stopped */
   size_t off_grad_pix;   /* f32[num_pix*3] dL/dpixel (loss gradient) */
   size_t off_slab_loss;  /* f32[num_items*slabs_per_tile] partial L2 losses */
   size_t off_grad2d;     /* float4[V*N*3] per-view 2D gradients */
@@ -183,14 +191,14 @@ typedef struct {
 int dsplat_gauss_batch_layout(int64_t num_pnt, int32_t num_views, const dsplat_view* views, int32_t tile_size,
                               uint64_t pair_capacity, dsplat_batch_layout* out);
 
-/* Forward over all views: projection (+SH), depth sort, pair emission, tile
- * sort, ranges and rasterisation in one launch sequence, no host sync (CUDA-
- * graph capturable).  out_rgb: concatenated [H_v,W_v,3] images; out_alpha
+/* Forward over all views: projection (+SH), depth sort, superblock lists and
+ * rasterisation in one launch sequence, no host sync (CUDA-graph
+ * capturable).  capacity: superblock-list entries (see _status).  out_rgb: concatenated [H_v,W_v,3] images; out_alpha
  * (nullable): 1 - T per pixel.  target (nullable, same layout as out_rgb):
  * also computes the L2 loss sum (per-item partials in the workspace) and
  * its pixel gradient for dsplat_gauss_batch_backward. */
 int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* params, int32_t num_views,
-                               const dsplat_view* views, int32_t tile_size, uint64_t pair_capacity, void* workspace,
+                               const dsplat_view* views, int32_t tile_size, uint64_t capacity, void* workspace,
                                size_t workspace_bytes, float* out_rgb, float* out_alpha, const float* target);
 
 /* Backward of the last forward on this workspace.  grad_rgb (nullable):
@@ -199,9 +207,11 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
                                 const dsplat_view* views, int32_t tile_size, uint64_t pair_capacity, void* workspace,
                                 size_t workspace_bytes, const float* grad_rgb, const dsplat_gauss_grads* grads);
 
-/* Synchronises the stream and reports the overflow flag and the pair total of
- * the last forward (a capacity overflow leaves outputs undefined). */
-int dsplat_gauss_batch_status(dsplat_stream stream, const void* workspace, uint32_t* flags, uint64_t* num_pairs);
+/* Synchronises the stream and reports, for the last forward, the flags (bit 0:
+ * capacity overflow -- outputs undefined), the capacity it needed (superblock
+ * entries) and its number of (tile, point) pairs. */
+int dsplat_gauss_batch_status(dsplat_stream stream, const void* workspace, uint32_t* flags, uint64_t* capacity_needed,
+                              uint64_t* tile_pairs);
 
 /* Profiling hook: CUDA events (cudaEvent_t) recorded on the launch stream at
  * the stage boundaries of the batched calls on this host thread:

@@ -35,12 +35,9 @@ def _run(orc, dev, sc, target, ts=16):
     rec = F(batch.records()[0])
     aabb = np.stack([rec[:, 0] - rec[:, 9], rec[:, 1] - rec[:, 10], rec[:, 0] + rec[:, 9],
                      rec[:, 1] + rec[:, 10]], 1).astype(np.float32)
-    t2i, i2p = batch.tile_lists(0)
-    starts = batch._ws(batch.layout.off_item_start, int(batch.layout.num_items) + 1, torch.int32)
-    last = F(batch.per_pixel("stop")[0]).astype(np.int64) - int(starts[0])
+    t2i, i2p, last = batch.tile_lists(0)
     S = orc.Scene(sc.means, sc.log_scales, sc.quats, sc.opacity, sc.colors.reshape(sc.n, -1), sc.sh_degree,
-                  cam.mvp, cam.campos, cam.width, cam.height, ts, U32(t2i), U32(i2p), last.astype(np.int32), aabb,
-                  target)
+                  cam.mvp, cam.campos, cam.width, cam.height, ts, t2i, i2p, last.astype(np.int32), aabb, target)
     return batch, {k: F(v).reshape(sc.n, -1).astype(np.float64) for k, v in grads.items()}, S
 
 
@@ -66,7 +63,7 @@ def test_gradients_small(orc, dev, sh_deg):
         ok = _close(g_gpu[k], ref, scale, 1e-3, 1e-2)
         assert ok.mean() > 0.999, (k, ok.mean(), np.abs(g_gpu[k] - ref).max(), scale)
     # FD on 64 random parameters of visible Gaussians
-    vis = np.unique(U32(batch.tile_lists(0)[1]))
+    vis = np.unique(batch.tile_lists(0)[1])
     picks = []
     for _ in range(64):
         k = GROUPS[rng.integers(0, len(GROUPS))]
