@@ -126,12 +126,10 @@ __device__ __forceinline__ float quad(float B, float C, float dx, float dy, floa
 }
 
 // ---------------------------------------------------------------------------
-// Forward walk of one slab by one warp over the list range [s, e).
-// Every pixel slot of a lane is evaluated branch-free: a slot that is done or
-// outside the entry's box gets alpha = 0, which leaves colour, T and
-// alpha_sum bit-for-bit unchanged (x*0 = +-0 and y + +-0 = y), so the result
-// equals the reference's skip-and-break walk while the 8 slots run in
-// parallel (instruction-level parallelism).
+// Forward walk of one slab by one warp over the list range [s, e).  Slot k of
+// every lane lies in the same row pair of the slab, so the per-slot skips
+// (pixel done, row outside the entry's box) are uniform across the warp most
+// of the time.
 // ---------------------------------------------------------------------------
 template <int TS, class Walk, class Src>
 __device__ __forceinline__ void fwd_slab(const Walk& walk, const Src& src, Ent* sm, uint32_t s, uint32_t e, int px0,
@@ -176,26 +174,23 @@ __device__ __forceinline__ void fwd_slab(const Walk& walk, const Src& src, Ent* 
         if (!(ec.y <= fx && fx <= ec.w)) continue;
         const float dx = fs(fx, ea.x);
         const float adxdx = fm(fm(ea.z, dx), dx);
-        float al[PPL];
-#pragma unroll
-        for (int k = 0; k < PPL; ++k) {
-          const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
-          const bool act = ((live >> k) & 1u) && ec.z <= fy && fy <= ed.x;
-          const float dy = fs(fy, ea.y);
-          const float q = quad(ea.w, eb.x, dx, dy, adxdx);
-          const float a = fm(dexp(fm(-0.5f, q)), eb.y);
-          al[k] = act ? a : 0.f;
-        }
         const uint32_t pos = __float_as_uint(ed.z);
 #pragma unroll
         for (int k = 0; k < PPL; ++k) {
-          const float eo = fm(T[k], al[k]);
+          // a slot is one row pair across the warp: the skip is warp-uniform in practice
+          if (!((live >> k) & 1u)) continue;
+          const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
+          if (!(ec.z <= fy && fy <= ed.x)) continue;
+          const float dy = fs(fy, ea.y);
+          const float q = quad(ea.w, eb.x, dx, dy, adxdx);
+          const float al = fm(dexp(fm(-0.5f, q)), eb.y);
+          const float eo = fm(T[k], al);
           c0[k] = fa(c0[k], fm(eb.z, eo));
           c1[k] = fa(c1[k], fm(eb.w, eo));
           c2[k] = fa(c2[k], fm(ec.x, eo));
-          T[k] = fm(T[k], fs(1.f, al[k]));
+          T[k] = fm(T[k], fs(1.f, al));
           as[k] = fa(as[k], eo);
-          if (((live >> k) & 1u) && as[k] >= kAlphaBreak) {
+          if (as[k] >= kAlphaBreak) {
             live &= ~(1u << k);
             last[k] = pos;
           }
@@ -312,10 +307,9 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
 // ---------------------------------------------------------------------------
 // Fused-path backward.  grad2d[(v*N+g)*3 + k] float4:
 //   (d px, d py, d A, d B) (d C, d opacity, d r, d g) (d b, 0, 0, 0)
-// Inactive slots get G = 0, which makes every update below a no-op, so the
-// 8 slots are evaluated branch-free.  exp and 1/(1-alpha) use the hardware
-// approximations: gradients need not reproduce the forward bit for bit (the
-// discrete structure -- boxes, stop positions -- comes from the forward).
+// exp and 1/(1-alpha) use the hardware approximations: gradients need not
+// reproduce the forward bit for bit (the discrete structure -- boxes, stop
+// positions -- comes from the forward).
 // ---------------------------------------------------------------------------
 template <int TS>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
@@ -382,11 +376,11 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
 #pragma unroll
           for (int k = 0; k < PPL; ++k) {
             const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
-            const bool act = pos >= last[k] && ec.z <= fy && fy <= ed.x;
-            any |= act;
+            if (pos < last[k] || !(ec.z <= fy && fy <= ed.x)) continue;
+            any = true;
             const float dy = fs(fy, ea.y);
             const float q = quad(B, C, dx, dy, adxdx);
-            const float Gv = act ? __expf(-0.5f * q) : 0.f;
+            const float Gv = __expf(-0.5f * q);
             const float al = Gv * op;
             const float iom = __frcp_rn(1.f - al);
             Tc[k] = Tc[k] * iom;
