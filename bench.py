@@ -183,6 +183,7 @@ def main():
     ap.add_argument("--n", type=int, default=1 << 20)
     ap.add_argument("--views", type=int, default=16)
     ap.add_argument("--tile", type=int, default=16)
+    ap.add_argument("--ppl", type=int, default=0, help="rasteriser pixels per lane (0: default)")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -211,7 +212,7 @@ def main():
     target = torch.from_numpy(np.concatenate([t.reshape(-1) for t in tgt_np])).to(dev)
     grads = {k: torch.zeros_like(v) for k, v in params.items()}
 
-    batch = GaussBatch(base.n, cams, args.tile, 3, pair_capacity=1 << 24, device=dev)
+    batch = GaussBatch(base.n, cams, args.tile, 3, pair_capacity=1 << 24, device=dev, pixels_per_lane=args.ppl)
     pairs = batch.ensure_capacity(params)
     V = len(cams)
     pix_off = batch.pix_offsets
@@ -228,7 +229,7 @@ def main():
     plain = []
     if not args.no_plain:
         for v, c in enumerate(cams):
-            b = GaussBatch(base.n, [c], args.tile, 3, pair_capacity=1 << 22, device=dev)
+            b = GaussBatch(base.n, [c], args.tile, 3, pair_capacity=1 << 22, device=dev, pixels_per_lane=args.ppl)
             b.ensure_capacity(params)
             plain.append((b, target[3 * pix_off[v]: 3 * pix_off[v + 1]]))
 
@@ -321,21 +322,22 @@ def main():
     # roofline of the dominant kernel (algorithmic bytes per launch / event time)
     peak, peak_kind = peaks()
     npix = int(batch.layout.num_pix)
-    names = ["project_fwd", "depth_sort", "tile_lists", "(unused)", "raster_fwd", "(host gap)",
+    names = ["project_fwd", "depth_sort", "sb_lists", "task_order", "raster_fwd", "(host gap)",
              "grad_clear", "raster_bwd", "project_bwd"]
     s_sh = 48
     bytes_alg = {
         "project_fwd": base.n * (40 + 4 + 4 * s_sh) + V * base.n * (48 + 8 + 4 + 4),
         "depth_sort": 4 * V * batch.layout.npad * 16,
-        "(unused)": 0,
-        "tile_lists": pairs * 4 + 2 * V * batch.layout.npad * 12,
+        "task_order": 0,
+        "sb_lists": 2 * V * batch.layout.npad * 12,
         "raster_fwd": pairs * 40 + npix * 20,
         "raster_bwd": npix * 20 + pairs * 40 + V * base.n * 36,
         "project_bwd": base.n * (40 + 4 * s_sh) + V * base.n * 48 + base.n * (40 + 4 * s_sh),
         "grad_clear": V * base.n * 48,
         "(host gap)": 0,
     }
-    dom = max((n for n in names if not n.startswith("(")), key=lambda n: stage_ms[names.index(n)])
+    dom = max((n for n in names if not n.startswith("(") and n != "task_order"),
+              key=lambda n: stage_ms[names.index(n)])
     dom_ms = stage_ms[names.index(dom)]
     achieved = bytes_alg[dom] / (dom_ms / 1e3) / 1e9
 
@@ -358,6 +360,7 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG64; no public dataset)",
             "config": {"workload": "1M Gaussians SH3, 16 views mixed 320x240..1920x1080, fwd+bwd, L2 loss",
                        "num_gaussians": base.n, "views_per_gpu": V, "tile_size": args.tile,
+                       "pixels_per_lane": batch.ppl or None,
                        "pairs_per_step": int(pairs_now), "pixels_per_step": npix,
                        "plain_views_per_s": plain_vps,
                        "batched_over_plain": (value / world) / (plain_vps / world) if plain_vps else None,

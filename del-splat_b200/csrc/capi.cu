@@ -42,10 +42,14 @@ size_t radix_hist_words(size_t n);
 cudaError_t exclusive_scan(cudaStream_t, const uint32_t*, uint32_t*, size_t, uint32_t*);
 cudaError_t radix_sort(cudaStream_t, uint32_t*, uint32_t*, uint32_t*, uint32_t*, size_t, const uint32_t*, int, uint32_t,
                        uint32_t*, uint32_t*, bool*);
-cudaError_t raster_fwd(cudaStream_t, const ViewBatch&, uint32_t, const float4*, const uint2*, const uint32_t*, uint32_t,
-                       uint64_t, uint32_t*, float*, float*, uint32_t*, const float*, float*, float*);
-cudaError_t raster_bwd(cudaStream_t, const ViewBatch&, uint32_t, const float4*, const uint2*, const uint32_t*, uint32_t,
-                       uint64_t, uint32_t*, const float*, const float*, const uint32_t*, float4*);
+cudaError_t raster_fwd(cudaStream_t, const ViewBatch&, const FwdArgs&);
+cudaError_t raster_bwd(cudaStream_t, const ViewBatch&, const BwdArgs&);
+bool raster_config_ok(int ts, int ppl);
+int raster_default_ppl(int ts);
+uint32_t raster_slabs_per_tile(int ts, int ppl);
+__global__ void k_order_hist(const ViewBatch, const uint32_t*, uint32_t, uint32_t*);
+__global__ void k_order_scan(uint32_t*);
+__global__ void k_order_scatter(const ViewBatch, const uint32_t*, uint32_t, uint32_t*, uint32_t*);
 cudaError_t raster_fwd_aos(cudaStream_t, int, int, int, float*, const float*, const float*, const float*, const float*,
                            const float*, const uint32_t*, const uint32_t*, float*, uint32_t*);
 cudaError_t circle_splat_tiles(cudaStream_t, int, int, int, float*, const float*, const float*, const float*,
@@ -209,6 +213,7 @@ ViewBatch single_view_batch(int w, int h, int ts, uint32_t tile_w, uint32_t tile
   memset(&b, 0, sizeof(b));
   b.num_views = 1;
   b.ts = ts;
+  b.ppl = raster_default_ppl(ts);
   b.num_items = tile_w * tile_h;
   b.num_pix = uint32_t(w) * uint32_t(h);
   b.v[0].w = w;
@@ -322,16 +327,21 @@ struct BatchWs {
   float* grad_pix;
   float* slab_loss;
   float4* grad2d;
+  uint32_t *sched, *task_order;
 };
 
-int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, ViewBatch* b) {
+int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, int32_t ppl, ViewBatch* b) {
   if (nv < 1 || nv > DSPLAT_MAX_VIEWS) return fail(DSPLAT_ERR_INVALID_ARG, "num_views must be in [1, 32]");
   if (!views) return fail(DSPLAT_ERR_INVALID_ARG, "views is null");
   if (!ts_ok(uint32_t(ts))) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
+  if (ppl == 0) ppl = raster_default_ppl(ts);
+  if (!raster_config_ok(ts, ppl))
+    return fail(DSPLAT_ERR_UNSUPPORTED, "pixels_per_lane must be 2 (8x8 tiles), 2/4/8 (16x16) or 4/8 (32x32)");
   if (n64 < 0 || n64 > int64_t(0x7fffffff)) return fail(DSPLAT_ERR_INVALID_ARG, "num_pnt out of range");
   memset(b, 0, sizeof(*b));
   b->num_views = nv;
   b->ts = ts;
+  b->ppl = ppl;
   uint64_t items = 0, pix = 0;
   for (int v = 0; v < nv; ++v) {
     const dsplat_view& s = views[v];
@@ -370,7 +380,7 @@ BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity)
   L.num_items = b.num_items;
   L.num_pix = b.num_pix;
   L.npad = npad;
-  L.slabs_per_tile = b.ts == 32 ? 4u : 1u;
+  L.slabs_per_tile = raster_slabs_per_tile(b.ts, b.ppl);
   w.flags = c.take<uint32_t>(16, &L.off_flags);
   w.rec = c.take<float4>(3 * VN + 3, &L.off_rec);
   w.rect = c.take<uint2>(VN + 1, &L.off_rect);
@@ -392,6 +402,8 @@ BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity)
   w.grad_pix = c.take<float>(size_t(b.num_pix) * 3, &L.off_grad_pix);
   w.slab_loss = c.take<float>(size_t(b.num_items) * L.slabs_per_tile, &L.off_slab_loss);
   w.grad2d = c.take<float4>(3 * VN + 3, &L.off_grad2d);
+  w.sched = c.take<uint32_t>(80);
+  w.task_order = c.take<uint32_t>(size_t(b.num_items) + 1);
   L.total_bytes = align_up(c.off, 256);
   return w;
 }
@@ -559,22 +571,23 @@ int dsplat_point_rasterize_pix(dsplat_stream stream, uint32_t num_pnt, const flo
 }
 
 int dsplat_gauss_batch_layout(int64_t num_pnt, int32_t num_views, const dsplat_view* views, int32_t tile_size,
-                              uint64_t pair_capacity, dsplat_batch_layout* out) {
+                              int32_t pixels_per_lane, uint64_t pair_capacity, dsplat_batch_layout* out) {
   if (!out) return fail(DSPLAT_ERR_INVALID_ARG, "out is null");
   ViewBatch b;
-  int rc = make_batch(num_pnt, num_views, views, tile_size, &b);
+  int rc = make_batch(num_pnt, num_views, views, tile_size, pixels_per_lane, &b);
   if (rc) return rc;
   *out = carve_batch(nullptr, uint32_t(num_pnt), b, pair_capacity).L;
   return DSPLAT_OK;
 }
 
 int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* params, int32_t num_views,
-                               const dsplat_view* views, int32_t tile_size, uint64_t pair_capacity, void* workspace,
-                               size_t workspace_bytes, float* out_rgb, float* out_alpha, const float* target) {
+                               const dsplat_view* views, int32_t tile_size, int32_t pixels_per_lane,
+                               uint64_t pair_capacity, void* workspace, size_t workspace_bytes, float* out_rgb,
+                               float* out_alpha, const float* target) {
   int rc = check_params(params);
   if (rc) return rc;
   ViewBatch b;
-  rc = make_batch(params->num_pnt, num_views, views, tile_size, &b);
+  rc = make_batch(params->num_pnt, num_views, views, tile_size, pixels_per_lane, &b);
   if (rc) return rc;
   if (pair_capacity > 0xfffff000ull) return fail(DSPLAT_ERR_INVALID_ARG, "pair_capacity must fit in u32");
   const uint32_t n = uint32_t(params->num_pnt);
@@ -605,9 +618,18 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
     if (rc2) return rc2;
     stage_mark(st, 3);
   }
+  // longest-first raster task order
+  TRY_CUDA(cudaMemsetAsync(w.sched, 0, 80 * sizeof(uint32_t), st), "memset");
+  k_order_hist<<<64, 256, 0, st>>>(b, w.lists.off1, npad / kChunk, w.sched);
+  count_launch();
+  k_order_scan<<<1, 32, 0, st>>>(w.sched);
+  count_launch();
+  k_order_scatter<<<64, 256, 0, st>>>(b, w.lists.off1, npad / kChunk, w.sched, w.task_order);
+  count_launch();
   stage_mark(st, 4);
-  TRY_CUDA(raster_fwd(st, b, n, w.rec, w.lists.list1, w.lists.off1, npad / kChunk, pair_capacity, w.flags + 2, out_rgb,
-                      w.pix_T, w.pix_stop, target, w.grad_pix, w.slab_loss),
+  const FwdArgs fa{n,        w.rec,        w.lists.list1, w.lists.off1, npad / kChunk, pair_capacity, w.task_order,
+                   w.flags + 2, out_rgb, w.pix_T,        w.pix_stop,   target,        w.grad_pix,    w.slab_loss};
+  TRY_CUDA(raster_fwd(st, b, fa),
            "raster_fwd");
   stage_mark(st, 5);
   if (out_alpha) {
@@ -619,15 +641,16 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
 }
 
 int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params* params, int32_t num_views,
-                                const dsplat_view* views, int32_t tile_size, uint64_t pair_capacity, void* workspace,
-                                size_t workspace_bytes, const float* grad_rgb, const dsplat_gauss_grads* grads) {
+                                const dsplat_view* views, int32_t tile_size, int32_t pixels_per_lane,
+                                uint64_t pair_capacity, void* workspace, size_t workspace_bytes, const float* grad_rgb,
+                                const dsplat_gauss_grads* grads) {
   int rc = check_params(params);
   if (rc) return rc;
   if (!grads || (params->num_pnt > 0 && (!grads->means || !grads->log_scales || !grads->quats || !grads->opacity ||
                                          !grads->colors)))
     return fail(DSPLAT_ERR_INVALID_ARG, "null gradient pointer");
   ViewBatch b;
-  rc = make_batch(params->num_pnt, num_views, views, tile_size, &b);
+  rc = make_batch(params->num_pnt, num_views, views, tile_size, pixels_per_lane, &b);
   if (rc) return rc;
   const uint32_t n = uint32_t(params->num_pnt);
   BatchWs w = carve_batch(nullptr, n, b, pair_capacity);
@@ -640,8 +663,9 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
   TRY_CUDA(cudaMemsetAsync(w.grad2d, 0, 3 * VN * sizeof(float4), st), "memset");
   TRY_CUDA(cudaMemsetAsync(w.flags + 3, 0, sizeof(uint32_t), st), "memset");
   stage_mark(st, 7);
-  TRY_CUDA(raster_bwd(st, b, n, w.rec, w.lists.list1, w.lists.off1, w.L.npad / kChunk, pair_capacity, w.flags + 3,
-                      grad_rgb ? grad_rgb : w.grad_pix, w.pix_T, w.pix_stop, w.grad2d),
+  const BwdArgs ba{n,           w.rec,    w.lists.list1,  w.lists.off1, w.L.npad / kChunk, pair_capacity,
+                   w.task_order, w.flags + 3, grad_rgb ? grad_rgb : w.grad_pix, w.pix_T, w.pix_stop, w.grad2d};
+  TRY_CUDA(raster_bwd(st, b, ba),
            "raster_bwd");
   stage_mark(st, 8);
   k_project_bwd<<<blocks_for(n, 128), 128, 0, st>>>(n, params->sh_degree, params->means, params->log_scales,

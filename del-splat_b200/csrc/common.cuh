@@ -35,8 +35,45 @@ struct ViewBatch {
   uint32_t num_pix;    // sum of pixel counts
   uint32_t num_sb;     // sum of superblock counts
   uint32_t max_sb;     // largest per-view superblock count
+  int32_t ppl;         // rasteriser pixels per lane (warp task = 32 * ppl pixels)
+  int32_t pad;
   ViewDev v[DSPLAT_MAX_VIEWS];
 };
+
+// Arguments of the fused rasteriser launches (host side).
+struct FwdArgs {
+  uint32_t n;
+  const float4* rec;
+  const uint2* list1;
+  const uint32_t* off1;
+  uint32_t nchunk;
+  uint64_t capacity;
+  const uint32_t* order;
+  uint32_t* counter;
+  float* out_rgb;
+  float* out_T;
+  uint32_t* out_last;
+  const float* target;
+  float* grad_pix;
+  float* slab_loss;
+};
+
+struct BwdArgs {
+  uint32_t n;
+  const float4* rec;
+  const uint2* list1;
+  const uint32_t* off1;
+  uint32_t nchunk;
+  uint64_t capacity;
+  const uint32_t* order;
+  uint32_t* counter;
+  const float* grad_pix;
+  const float* pix_T;
+  const uint32_t* pix_last;
+  float4* grad2d;
+};
+
+
 
 __device__ __forceinline__ int view_of_item(const ViewBatch& b, uint32_t item) {
   int v = 0;

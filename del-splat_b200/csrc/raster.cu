@@ -44,9 +44,9 @@ struct Ent {  // one staged list entry (64 bytes)
   float4 d;   // box y1, point index (bits), -, -
 };
 
-template <int TS>
+template <int TS, int PPL_>
 struct Geo {
-  static constexpr int PPL = TS == 8 ? 2 : 8;   // pixels per lane
+  static constexpr int PPL = PPL_;                // pixels per lane
   static constexpr int ROW_STEP = 32 / TS;        // rows covered by the 32 lanes at once
   static constexpr int SLAB_ROWS = ROW_STEP * PPL;
   static constexpr int SLABS = TS / SLAB_ROWS;    // warp tasks per tile
@@ -131,13 +131,13 @@ __device__ __forceinline__ float quad(float B, float C, float dx, float dy, floa
 // (pixel done, row outside the entry's box) are uniform across the warp most
 // of the time.
 // ---------------------------------------------------------------------------
-template <int TS, class Walk, class Src>
+template <int TS, int PPL_, class Walk, class Src>
 __device__ __forceinline__ void fwd_slab(const Walk& walk, const Src& src, Ent* sm, uint32_t s, uint32_t e, int px0,
                                          int py0, int w, int h, bool accumulate, float* __restrict__ out_rgb,
                                          size_t pix_base, float* __restrict__ out_T, uint32_t* __restrict__ out_last,
                                          const float* __restrict__ target, float* __restrict__ grad_pix,
                                          float* __restrict__ loss_slot) {
-  using G = Geo<TS>;
+  using G = Geo<TS, PPL_>;
   constexpr int PPL = G::PPL;
   const int lane = threadIdx.x & 31;
   const int ix = px0 + (lane % TS);
@@ -257,13 +257,14 @@ __device__ __forceinline__ ItemGeo item_geo(const ViewBatch& b, uint32_t item, c
 // walking each tile's entries out of its superblock list.
 // slab_loss: one partial L2 loss per task (when target is given).
 // ---------------------------------------------------------------------------
-template <int TS>
+template <int TS, int PPL>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint2* __restrict__ list1,
-    const uint32_t* __restrict__ off1, uint32_t nchunk, uint64_t capacity, uint32_t* __restrict__ work_counter,
-    float* __restrict__ out_rgb, float* __restrict__ out_T, uint32_t* __restrict__ out_last,
-    const float* __restrict__ target, float* __restrict__ grad_pix, float* __restrict__ slab_loss) {
-  using G = Geo<TS>;
+    const uint32_t* __restrict__ off1, uint32_t nchunk, uint64_t capacity, const uint32_t* __restrict__ order,
+    uint32_t* __restrict__ work_counter, float* __restrict__ out_rgb, float* __restrict__ out_T,
+    uint32_t* __restrict__ out_last, const float* __restrict__ target, float* __restrict__ grad_pix,
+    float* __restrict__ slab_loss) {
+  using G = Geo<TS, PPL>;
   __shared__ Ent sm_all[kRasterWarps][32];
   Ent* sm = sm_all[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -273,25 +274,26 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     if (lane == 0) task = atomicAdd(work_counter, 1u);
     task = __shfl_sync(0xffffffffu, task, 0);
     if (task >= num_tasks) return;
-    const uint32_t item = task / G::SLABS, slab = task % G::SLABS;
+    const uint32_t item = order[task / G::SLABS], slab = task % G::SLABS;
     const ItemGeo ig = item_geo(b, item, off1, nchunk, capacity);
     const ViewDev& vd = b.v[ig.v];
     PackedSrc src{rec + 3 * size_t(ig.v) * n};
     SbWalk walk{list1, ig.lx, ig.ly};
-    fwd_slab<TS>(walk, src, sm, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, false, out_rgb,
-                 vd.pix_base, out_T, out_last, target, grad_pix, slab_loss ? slab_loss + task : nullptr);
+    fwd_slab<TS, PPL>(walk, src, sm, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, false,
+                      out_rgb, vd.pix_base, out_T, out_last, target, grad_pix,
+                      slab_loss ? slab_loss + size_t(item) * G::SLABS + slab : nullptr);
     __syncwarp();
   }
 }
 
 // Drop-in forward (splat_gauss.rs:46-94): AoS inputs and per-tile lists,
 // accumulates into pix2rgb.
-template <int TS>
+template <int TS, int PPL>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
     int w, int h, int tile_w, uint32_t num_tasks, float* __restrict__ pix2rgb, AosSrc src,
     const uint32_t* __restrict__ tile2idx, const uint32_t* __restrict__ idx2pnt, float* __restrict__ out_T,
     uint32_t* __restrict__ out_last) {
-  using G = Geo<TS>;
+  using G = Geo<TS, PPL>;
   __shared__ Ent sm_all[kRasterWarps][32];
   Ent* sm = sm_all[threadIdx.x >> 5];
   const uint32_t task = blockIdx.x * kRasterWarps + (threadIdx.x >> 5);
@@ -300,8 +302,8 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
   const int px0 = int(tile % uint32_t(tile_w)) * TS;
   const int py0 = int(tile / uint32_t(tile_w)) * TS + int(slab) * G::SLAB_ROWS;
   TileWalk walk{idx2pnt};
-  fwd_slab<TS>(walk, src, sm, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, true, pix2rgb, 0, out_T, out_last,
-               nullptr, nullptr, nullptr);
+  fwd_slab<TS, PPL>(walk, src, sm, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, true, pix2rgb, 0, out_T,
+                    out_last, nullptr, nullptr, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -311,13 +313,13 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
 // reproduce the forward bit for bit (the discrete structure -- boxes, stop
 // positions -- comes from the forward).
 // ---------------------------------------------------------------------------
-template <int TS>
+template <int TS, int PPL_>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint2* __restrict__ list1,
-    const uint32_t* __restrict__ off1, uint32_t nchunk, uint64_t capacity, uint32_t* __restrict__ work_counter,
-    const float* __restrict__ grad_pix, const float* __restrict__ pix_T, const uint32_t* __restrict__ pix_last,
-    float4* __restrict__ grad2d) {
-  using G = Geo<TS>;
+    const uint32_t* __restrict__ off1, uint32_t nchunk, uint64_t capacity, const uint32_t* __restrict__ order,
+    uint32_t* __restrict__ work_counter, const float* __restrict__ grad_pix, const float* __restrict__ pix_T,
+    const uint32_t* __restrict__ pix_last, float4* __restrict__ grad2d) {
+  using G = Geo<TS, PPL_>;
   constexpr int PPL = G::PPL;
   __shared__ Ent sm_all[kRasterWarps][32];
   Ent* sm = sm_all[threadIdx.x >> 5];
@@ -328,7 +330,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     if (lane == 0) task = atomicAdd(work_counter, 1u);
     task = __shfl_sync(0xffffffffu, task, 0);
     if (task >= num_tasks) return;
-    const uint32_t item = task / G::SLABS, slab = task % G::SLABS;
+    const uint32_t item = order[task / G::SLABS], slab = task % G::SLABS;
     const ItemGeo ig = item_geo(b, item, off1, nchunk, capacity);
     const ViewDev& vd = b.v[ig.v];
     const int ix = ig.px0 + (lane % TS);
@@ -488,7 +490,13 @@ static int num_sms() {
   return sms;
 }
 
-uint32_t raster_slabs_per_tile(int ts) { return ts == 32 ? 4u : 1u; }
+// Supported (tile size, pixels per lane) pairs; slabs per tile follow.
+bool raster_config_ok(int ts, int ppl) {
+  return (ts == 8 && ppl == 2) || (ts == 16 && (ppl == 2 || ppl == 4 || ppl == 8)) ||
+         (ts == 32 && (ppl == 4 || ppl == 8));
+}
+int raster_default_ppl(int ts) { return ts == 8 ? 2 : 4; }
+uint32_t raster_slabs_per_tile(int ts, int ppl) { return uint32_t(ts * ts / (32 * ppl)); }
 
 template <class K>
 static int persistent_grid(K kernel, uint32_t tasks) {
@@ -501,104 +509,77 @@ static int persistent_grid(K kernel, uint32_t tasks) {
   return g < 1 ? 1 : g;
 }
 
-template <int TS>
-static void launch_fwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint2* list1,
-                       const uint32_t* off1, uint32_t nchunk, uint64_t capacity, uint32_t* counter, float* out_rgb,
-                       float* out_T, uint32_t* out_last, const float* target, float* grad_pix, float* slab_loss) {
-  static int grid = 0;
-  static uint32_t cached_tasks = 0;
-  const uint32_t tasks = b.num_items * Geo<TS>::SLABS;
-  if (!grid || cached_tasks != tasks) {
-    grid = persistent_grid(k_raster_fwd<TS>, tasks);
-    cached_tasks = tasks;
-  }
-  k_raster_fwd<TS><<<grid, 32 * kRasterWarps, 0, st>>>(b, n, rec, list1, off1, nchunk, capacity, counter, out_rgb,
-                                                       out_T, out_last, target, grad_pix, slab_loss);
+template <int TS, int PPL>
+static void launch_fwd(cudaStream_t st, const ViewBatch& b, const FwdArgs& a) {
+  const uint32_t tasks = b.num_items * Geo<TS, PPL>::SLABS;
+  k_raster_fwd<TS, PPL><<<persistent_grid(k_raster_fwd<TS, PPL>, tasks), 32 * kRasterWarps, 0, st>>>(
+      b, a.n, a.rec, a.list1, a.off1, a.nchunk, a.capacity, a.order, a.counter, a.out_rgb, a.out_T, a.out_last,
+      a.target, a.grad_pix, a.slab_loss);
   count_launch();
 }
 
-template <int TS>
-static void launch_bwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint2* list1,
-                       const uint32_t* off1, uint32_t nchunk, uint64_t capacity, uint32_t* counter,
-                       const float* grad_pix, const float* pix_T, const uint32_t* pix_last, float4* grad2d) {
-  static int grid = 0;
-  static uint32_t cached_tasks = 0;
-  const uint32_t tasks = b.num_items * Geo<TS>::SLABS;
-  if (!grid || cached_tasks != tasks) {
-    grid = persistent_grid(k_raster_bwd<TS>, tasks);
-    cached_tasks = tasks;
-  }
-  k_raster_bwd<TS><<<grid, 32 * kRasterWarps, 0, st>>>(b, n, rec, list1, off1, nchunk, capacity, counter, grad_pix,
-                                                       pix_T, pix_last, grad2d);
+template <int TS, int PPL>
+static void launch_bwd(cudaStream_t st, const ViewBatch& b, const BwdArgs& a) {
+  const uint32_t tasks = b.num_items * Geo<TS, PPL>::SLABS;
+  k_raster_bwd<TS, PPL><<<persistent_grid(k_raster_bwd<TS, PPL>, tasks), 32 * kRasterWarps, 0, st>>>(
+      b, a.n, a.rec, a.list1, a.off1, a.nchunk, a.capacity, a.order, a.counter, a.grad_pix, a.pix_T, a.pix_last,
+      a.grad2d);
   count_launch();
 }
 
-cudaError_t raster_fwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint2* list1,
-                       const uint32_t* off1, uint32_t nchunk, uint64_t capacity, uint32_t* counter, float* out_rgb,
-                       float* out_T, uint32_t* out_last, const float* target, float* grad_pix, float* slab_loss) {
-  switch (b.ts) {
-    case 8:
-      launch_fwd<8>(st, b, n, rec, list1, off1, nchunk, capacity, counter, out_rgb, out_T, out_last, target, grad_pix,
-                    slab_loss);
-      break;
-    case 16:
-      launch_fwd<16>(st, b, n, rec, list1, off1, nchunk, capacity, counter, out_rgb, out_T, out_last, target,
-                     grad_pix, slab_loss);
-      break;
-    case 32:
-      launch_fwd<32>(st, b, n, rec, list1, off1, nchunk, capacity, counter, out_rgb, out_T, out_last, target,
-                     grad_pix, slab_loss);
-      break;
-    default:
-      return cudaErrorInvalidValue;
+#define DSPLAT_RASTER_CONFIGS(X) X(8, 2) X(16, 2) X(16, 4) X(16, 8) X(32, 4) X(32, 8)
+
+cudaError_t raster_fwd(cudaStream_t st, const ViewBatch& b, const FwdArgs& a) {
+#define X(T, P)                        \
+  if (b.ts == T && b.ppl == P) {       \
+    launch_fwd<T, P>(st, b, a);        \
+    return cudaGetLastError();         \
   }
-  return cudaGetLastError();
+  DSPLAT_RASTER_CONFIGS(X)
+#undef X
+  return cudaErrorInvalidValue;
 }
 
-cudaError_t raster_bwd(cudaStream_t st, const ViewBatch& b, uint32_t n, const float4* rec, const uint2* list1,
-                       const uint32_t* off1, uint32_t nchunk, uint64_t capacity, uint32_t* counter,
-                       const float* grad_pix, const float* pix_T, const uint32_t* pix_last, float4* grad2d) {
-  switch (b.ts) {
-    case 8:
-      launch_bwd<8>(st, b, n, rec, list1, off1, nchunk, capacity, counter, grad_pix, pix_T, pix_last, grad2d);
-      break;
-    case 16:
-      launch_bwd<16>(st, b, n, rec, list1, off1, nchunk, capacity, counter, grad_pix, pix_T, pix_last, grad2d);
-      break;
-    case 32:
-      launch_bwd<32>(st, b, n, rec, list1, off1, nchunk, capacity, counter, grad_pix, pix_T, pix_last, grad2d);
-      break;
-    default:
-      return cudaErrorInvalidValue;
+cudaError_t raster_bwd(cudaStream_t st, const ViewBatch& b, const BwdArgs& a) {
+#define X(T, P)                        \
+  if (b.ts == T && b.ppl == P) {       \
+    launch_bwd<T, P>(st, b, a);        \
+    return cudaGetLastError();         \
   }
-  return cudaGetLastError();
+  DSPLAT_RASTER_CONFIGS(X)
+#undef X
+  return cudaErrorInvalidValue;
+}
+
+template <int TS, int PPL>
+static void launch_aos(cudaStream_t st, int w, int h, float* pix2rgb, const AosSrc& src, const uint32_t* tile2idx,
+                       const uint32_t* idx2pnt, float* out_T, uint32_t* out_last) {
+  const int tw = (w + TS - 1) / TS, th = (h + TS - 1) / TS;
+  const uint32_t tasks = uint32_t(tw) * uint32_t(th) * Geo<TS, PPL>::SLABS;
+  const unsigned grid = (tasks + kRasterWarps - 1) / kRasterWarps;
+  k_raster_fwd_aos<TS, PPL><<<grid, 32 * kRasterWarps, 0, st>>>(w, h, tw, tasks, pix2rgb, src, tile2idx, idx2pnt,
+                                                                out_T, out_last);
+  count_launch();
 }
 
 cudaError_t raster_fwd_aos(cudaStream_t st, int ts, int w, int h, float* pix2rgb, const float* xyd, const float* conic,
                            const float* aabb, const float* opacity, const float* rgb, const uint32_t* tile2idx,
                            const uint32_t* idx2pnt, float* out_T, uint32_t* out_last) {
-  const int tw = (w + ts - 1) / ts, th = (h + ts - 1) / ts;
-  if (tw == 0 || th == 0) return cudaSuccess;
-  const uint32_t tasks = uint32_t(tw) * uint32_t(th) * raster_slabs_per_tile(ts);
-  const unsigned grid = (tasks + kRasterWarps - 1) / kRasterWarps;
-  AosSrc src{xyd, conic, aabb, opacity, rgb};
+  if (w <= 0 || h <= 0) return cudaSuccess;
+  const AosSrc src{xyd, conic, aabb, opacity, rgb};
   switch (ts) {
     case 8:
-      k_raster_fwd_aos<8><<<grid, 32 * kRasterWarps, 0, st>>>(w, h, tw, tasks, pix2rgb, src, tile2idx, idx2pnt, out_T,
-                                                              out_last);
+      launch_aos<8, 2>(st, w, h, pix2rgb, src, tile2idx, idx2pnt, out_T, out_last);
       break;
     case 16:
-      k_raster_fwd_aos<16><<<grid, 32 * kRasterWarps, 0, st>>>(w, h, tw, tasks, pix2rgb, src, tile2idx, idx2pnt, out_T,
-                                                               out_last);
+      launch_aos<16, 4>(st, w, h, pix2rgb, src, tile2idx, idx2pnt, out_T, out_last);
       break;
     case 32:
-      k_raster_fwd_aos<32><<<grid, 32 * kRasterWarps, 0, st>>>(w, h, tw, tasks, pix2rgb, src, tile2idx, idx2pnt, out_T,
-                                                               out_last);
+      launch_aos<32, 4>(st, w, h, pix2rgb, src, tile2idx, idx2pnt, out_T, out_last);
       break;
     default:
       return cudaErrorInvalidValue;
   }
-  count_launch();
   return cudaGetLastError();
 }
 

@@ -535,6 +535,52 @@ __global__ void __launch_bounds__(kMsThreads) k_tile_scatter(const uint2* __rest
   }
 }
 
+// ---------------------------------------------------------------------------
+// Longest-first task order for the rasteriser: items bucketed by floor(log2)
+// of their superblock-list length, heaviest bucket first, so the tail of the
+// persistent launch is made of short tasks.  sched[0..31] counts, [32..63]
+// cursors.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t item_cost_bucket(const ViewBatch& b, uint32_t item, const uint32_t* off1,
+                                                     uint32_t nchunk) {
+  int v = 0;
+  for (int k = 1; k < b.num_views; ++k)
+    if (item >= b.v[k].item_base) v = k;
+  const ViewDev& vd = b.v[v];
+  const uint32_t t = item - vd.item_base;
+  const uint32_t tx = t % uint32_t(vd.tile_w), ty = t / uint32_t(vd.tile_w);
+  const uint32_t sb = vd.sb_base + (ty >> 3) * (uint32_t(vd.tile_w + 7) >> 3) + (tx >> 3);
+  const uint32_t len = off1[size_t(sb + 1) * nchunk] - off1[size_t(sb) * nchunk];
+  return len ? uint32_t(__clz(len)) : 32u;  // 0 = longest
+}
+
+__global__ void k_order_hist(const ViewBatch b, const uint32_t* __restrict__ off1, uint32_t nchunk,
+                             uint32_t* __restrict__ sched) {
+  __shared__ uint32_t h[33];
+  if (threadIdx.x < 33) h[threadIdx.x] = 0;
+  __syncthreads();
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.num_items; i += gridDim.x * blockDim.x)
+    atomicAdd(&h[item_cost_bucket(b, i, off1, nchunk)], 1u);
+  __syncthreads();
+  if (threadIdx.x < 33 && h[threadIdx.x]) atomicAdd(&sched[threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void k_order_scan(uint32_t* __restrict__ sched) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    uint32_t run = 0;
+    for (int k = 0; k < 33; ++k) {
+      sched[40 + k] = run;
+      run += sched[k];
+    }
+  }
+}
+
+__global__ void k_order_scatter(const ViewBatch b, const uint32_t* __restrict__ off1, uint32_t nchunk,
+                                uint32_t* __restrict__ sched, uint32_t* __restrict__ order) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.num_items; i += gridDim.x * blockDim.x)
+    order[atomicAdd(&sched[40 + item_cost_bucket(b, i, off1, nchunk)], 1u)] = i;
+}
+
 // Clamp tile ranges to the pair capacity after an overflow so that readers
 // stay in bounds (the results are then invalid and the flag is set).
 __global__ void k_clamp_ranges(uint32_t* __restrict__ item_start, uint32_t num_items, uint64_t capacity,

@@ -59,11 +59,12 @@ class GaussBatch:
     """
 
     def __init__(self, num_pnt: int, cameras: Sequence[Camera], tile_size: int = 16, sh_degree: int = 3,
-                 pair_capacity: int = 1 << 20, device: Optional[torch.device] = None):
+                 pair_capacity: int = 1 << 20, device: Optional[torch.device] = None, pixels_per_lane: int = 0):
         self.device = torch.device(device or "cuda")
         self.n = int(num_pnt)
         self.cameras = list(cameras)
         self.tile_size = int(tile_size)
+        self.ppl = int(pixels_per_lane)
         self.sh_degree = int(sh_degree)
         self.views = make_views(self.cameras)
         self.num_views = len(self.cameras)
@@ -74,7 +75,7 @@ class GaussBatch:
     def _alloc(self, capacity: int) -> None:
         self.capacity = max(1, capacity)
         L = N.BatchLayout()
-        N.check(N.lib().dsplat_gauss_batch_layout(self.n, self.num_views, self.views, self.tile_size,
+        N.check(N.lib().dsplat_gauss_batch_layout(self.n, self.num_views, self.views, self.tile_size, self.ppl,
                                                   self.capacity, ctypes.byref(L)), "batch_layout")
         self.layout = L
         self.ws = torch.empty(int(L.total_bytes), dtype=torch.uint8, device=self.device)
@@ -109,8 +110,8 @@ class GaussBatch:
         if target is not None:
             _require_cuda(target, "target")
         N.check(N.lib().dsplat_gauss_batch_forward(
-            _stream_ptr(self.device), ctypes.byref(ps), self.num_views, self.views, self.tile_size, self.capacity,
-            self.ws.data_ptr(), self.ws.numel(), out.data_ptr(),
+            _stream_ptr(self.device), ctypes.byref(ps), self.num_views, self.views, self.tile_size, self.ppl,
+            self.capacity, self.ws.data_ptr(), self.ws.numel(), out.data_ptr(),
             out_alpha.data_ptr() if out_alpha is not None else None,
             target.data_ptr() if target is not None else None), "batch_forward")
         return out
@@ -125,8 +126,8 @@ class GaussBatch:
         if grad_rgb is not None:
             _require_cuda(grad_rgb, "grad_rgb")
         N.check(N.lib().dsplat_gauss_batch_backward(
-            _stream_ptr(self.device), ctypes.byref(ps), self.num_views, self.views, self.tile_size, self.capacity,
-            self.ws.data_ptr(), self.ws.numel(), grad_rgb.data_ptr() if grad_rgb is not None else None,
+            _stream_ptr(self.device), ctypes.byref(ps), self.num_views, self.views, self.tile_size, self.ppl,
+            self.capacity, self.ws.data_ptr(), self.ws.numel(), grad_rgb.data_ptr() if grad_rgb is not None else None,
             ctypes.byref(gs)), "batch_backward")
 
     # ----------------------------------------------------------- views of the workspace

@@ -188,8 +188,12 @@ typedef struct {
   size_t off_grad2d;     /* float4[V*N*3] per-view 2D gradients */
 } dsplat_batch_layout;
 
+/* tile_size: 8, 16 or 32.  pixels_per_lane: rasteriser work split, one warp
+ * task covers 32 * pixels_per_lane pixels of a tile: 2 for 8x8 tiles, 2/4/8
+ * for 16x16, 4/8 for 32x32; 0 picks the default (2, 4, 4).  Both are
+ * throughput knobs only: results do not depend on pixels_per_lane. */
 int dsplat_gauss_batch_layout(int64_t num_pnt, int32_t num_views, const dsplat_view* views, int32_t tile_size,
-                              uint64_t pair_capacity, dsplat_batch_layout* out);
+                              int32_t pixels_per_lane, uint64_t capacity, dsplat_batch_layout* out);
 
 /* Forward over all views: projection (+SH), depth sort, superblock lists and
  * rasterisation in one launch sequence, no host sync (CUDA-graph
@@ -198,13 +202,15 @@ int dsplat_gauss_batch_layout(int64_t num_pnt, int32_t num_views, const dsplat_v
  * also computes the L2 loss sum (per-item partials in the workspace) and
  * its pixel gradient for dsplat_gauss_batch_backward. */
 int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* params, int32_t num_views,
-                               const dsplat_view* views, int32_t tile_size, uint64_t capacity, void* workspace,
+                               const dsplat_view* views, int32_t tile_size, int32_t pixels_per_lane,
+                               uint64_t capacity, void* workspace,
                                size_t workspace_bytes, float* out_rgb, float* out_alpha, const float* target);
 
 /* Backward of the last forward on this workspace.  grad_rgb (nullable):
  * dL/d out_rgb; null uses the L2-loss gradient stored by the forward. */
 int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params* params, int32_t num_views,
-                                const dsplat_view* views, int32_t tile_size, uint64_t pair_capacity, void* workspace,
+                                const dsplat_view* views, int32_t tile_size, int32_t pixels_per_lane,
+                                uint64_t capacity, void* workspace,
                                 size_t workspace_bytes, const float* grad_rgb, const dsplat_gauss_grads* grads);
 
 /* Synchronises the stream and reports, for the last forward, the flags (bit 0:

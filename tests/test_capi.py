@@ -39,10 +39,11 @@ def test_version_and_argument_checks_need_no_gpu():
     lay = N.BatchLayout()
     views = (N.View * 1)()
     views[0].width, views[0].height = 100, 50
-    assert L.dsplat_gauss_batch_layout(1000, 1, views, 16, 5000, ctypes.byref(lay)) == 0
+    assert L.dsplat_gauss_batch_layout(1000, 1, views, 16, 0, 5000, ctypes.byref(lay)) == 0
     assert lay.num_items == 7 * 4 and lay.num_pix == 5000 and lay.total_bytes > 0
-    assert L.dsplat_gauss_batch_layout(1000, 0, views, 16, 5000, ctypes.byref(lay)) == 1
-    assert L.dsplat_gauss_batch_layout(1000, 1, views, 24, 5000, ctypes.byref(lay)) == 5
+    assert L.dsplat_gauss_batch_layout(1000, 0, views, 16, 0, 5000, ctypes.byref(lay)) == 1
+    assert L.dsplat_gauss_batch_layout(1000, 1, views, 24, 0, 5000, ctypes.byref(lay)) == 5
+    assert L.dsplat_gauss_batch_layout(1000, 1, views, 16, 3, 5000, ctypes.byref(lay)) == 5
     assert L.dsplat_tile2idx_workspace_size(1000, 7, 4, 100) > L.dsplat_tile2idx_workspace_size(1000, 7, 4, 0)
 
 
@@ -52,6 +53,6 @@ def test_layout_grows_with_capacity_and_views():
     for i in range(2):
         v[i].width, v[i].height = 640, 480
     a, b = N.BatchLayout(), N.BatchLayout()
-    L.dsplat_gauss_batch_layout(10000, 1, v, 16, 1 << 16, ctypes.byref(a))
-    L.dsplat_gauss_batch_layout(10000, 2, v, 16, 1 << 20, ctypes.byref(b))
+    L.dsplat_gauss_batch_layout(10000, 1, v, 16, 0, 1 << 16, ctypes.byref(a))
+    L.dsplat_gauss_batch_layout(10000, 2, v, 16, 0, 1 << 20, ctypes.byref(b))
     assert b.total_bytes > a.total_bytes and b.num_items == 2 * a.num_items

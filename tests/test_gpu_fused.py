@@ -53,10 +53,11 @@ def _check_view(orc, batch, sc, v, ts):
     assert np.array_equal(stop, o_last)
 
 
-@pytest.mark.parametrize("sh_deg,ts", [(-1, 16), (0, 16), (1, 8), (3, 16), (3, 32)])
-def test_batched_forward_matches_oracle(orc, dev, sh_deg, ts):
+@pytest.mark.parametrize("sh_deg,ts,ppl", [(-1, 16, 0), (0, 16, 2), (1, 8, 2), (3, 16, 4), (3, 16, 8), (3, 32, 4),
+                                            (2, 32, 8)])
+def test_batched_forward_matches_oracle(orc, dev, sh_deg, ts, ppl):
     sc = _scene(sh_deg)
-    batch = GaussBatch(sc.n, sc.cameras, ts, sh_deg, pair_capacity=1000, device=dev)
+    batch = GaussBatch(sc.n, sc.cameras, ts, sh_deg, pair_capacity=1000, device=dev, pixels_per_lane=ppl)
     p = params_of(sc, dev)
     pairs = batch.ensure_capacity(p)
     assert pairs > 0 and batch.status()[0] == 0
