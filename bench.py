@@ -182,7 +182,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1 << 20)
     ap.add_argument("--views", type=int, default=16)
-    ap.add_argument("--tile", type=int, default=16)
+    ap.add_argument("--tile", type=int, default=8)
     ap.add_argument("--ppl", type=int, default=0, help="rasteriser pixels per lane (0: default)")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
