@@ -417,6 +417,11 @@ int check_params(const dsplat_gauss_params* p) {
 }
 
 }  // namespace
+
+// Records the message returned by dsplat_last_error() for entry points that
+// live in other translation units.
+int report_error(int code, const char* msg) { return fail(code, msg); }
+
 }  // namespace dsplat
 
 using namespace dsplat;

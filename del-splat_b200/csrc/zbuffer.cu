@@ -20,6 +20,8 @@
 // The all-ones key means "no point"; it can never be produced (low word <=
 // 0xFFFFFFFE).
 #include <cfloat>
+#include <cstdio>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -130,4 +132,82 @@ __global__ void k_circle_resolve(size_t npix, const uint64_t* __restrict__ zbuf,
   if (winner) winner[p] = int32_t(i);
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the point z-buffer.
+//
+// dsplat_point_rasterize_pix_zbuffer needs a W*H array of 64-bit keys from
+// the caller.  Some callers cannot provide one: a render plug-in whose host
+// application owns every device allocation and gives the library none, or a
+// real-time loop that may not call cudaMalloc (it can block the whole device)
+// and has no workspace to lend.  For them the keys live in this file-scope
+// device array instead: 2^20 keys (8 MiB), enough for 1024x1024 or 1280x720.
+// It is part of the module, so every GPU that loads libdsplat.so holds these
+// 8 MiB until the process exits.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocMaxPixels = size_t(1) << 20;
+static __device__ __align__(256) unsigned long long g_noalloc_zbuf[kNoAllocMaxPixels];
+
+int report_error(int code, const char* msg);
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of g_noalloc_zbuf on the current device (host code only sees
+// a host-side stand-in under that name).  Looked up once per device.
+int noalloc_scratch(uint64_t** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return report_error(DSPLAT_ERR_CUDA, "cudaGetDevice failed");
+  if (dev < 0 || dev >= kMaxDevices) return report_error(DSPLAT_ERR_UNSUPPORTED, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_zbuf);
+    if (e != cudaSuccess || !p) return report_error(DSPLAT_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_zbuf) failed");
+    g_noalloc_addr[dev] = p;
+  }
+  *out = static_cast<uint64_t*>(g_noalloc_addr[dev]);
+  return DSPLAT_OK;
+}
+}  // namespace
 }  // namespace dsplat
+
+// Same contract and results as dsplat_point_rasterize_pix_zbuffer, without the
+// zbuf argument: the keys are kept in the library's own 2^20-entry device
+// array.  Images larger than 2^20 pixels are rejected.  The first call on a
+// device looks the array up (cudaGetSymbolAddress) -- make that first call
+// before any stream capture.  All calls share the one array (it is refilled at
+// the start of every call), so calls whose GPU work overlaps -- on different
+// streams or host threads -- race and must be serialised by the caller.
+extern "C" int dsplat_point_rasterize_pix_zbuffer_noalloc(dsplat_stream stream, uint32_t num_pnt,
+                                                          const float* pnt2pixxyndcz, const float* pnt2rgb,
+                                                          float* pix2rgb, float* pix2unitdepth, int32_t* pix2winner,
+                                                          uint32_t img_w, uint32_t img_h) {
+  using namespace dsplat;
+  const size_t npix = size_t(img_w) * img_h;
+  if (npix == 0) return DSPLAT_OK;
+  if (npix > kNoAllocMaxPixels) {
+    char msg[160];
+    snprintf(msg, sizeof(msg), "image of %zu pixels exceeds the allocation-free z-buffer limit of %zu pixels", npix,
+             kNoAllocMaxPixels);
+    return report_error(DSPLAT_ERR_INVALID_ARG, msg);
+  }
+  if ((num_pnt > 0 && !pnt2pixxyndcz) || (pix2rgb && !pnt2rgb)) return report_error(DSPLAT_ERR_INVALID_ARG, "null pointer");
+  uint64_t* zbuf = nullptr;
+  const int rc = noalloc_scratch(&zbuf);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_fill_u64<<<unsigned((npix + 255) / 256), 256, 0, st>>>(zbuf, npix, ~0ull);
+  count_launch();
+  if (num_pnt > 0) {
+    k_point_zbuf<<<(num_pnt + 255) / 256, 256, 0, st>>>(num_pnt, pnt2pixxyndcz, int(img_w), int(img_h), zbuf);
+    count_launch();
+  }
+  k_point_resolve<<<unsigned((npix + 255) / 256), 256, 0, st>>>(npix, zbuf, pnt2pixxyndcz, pnt2rgb, pix2rgb,
+                                                                pix2unitdepth, pix2winner);
+  count_launch();
+  if (cudaGetLastError() != cudaSuccess) return report_error(DSPLAT_ERR_CUDA, "allocation-free point z-buffer launch");
+  return DSPLAT_OK;
+}

@@ -76,6 +76,7 @@ SIGNATURES = {
     "dsplat_circle_splat_zbuffer": (c_i32, [_P, c_u32, _P, _P, _P, c_i32, _P, _P, c_u32, c_u32, c_u32, _P]),
     "dsplat_point_rasterize_pix_zbuffer": (c_i32, [_P, c_u32, _P, _P, _P, _P, _P, c_u32, c_u32, _P]),
     "dsplat_point_rasterize_pix": (c_i32, [_P, c_u32, _P, _P, _P, c_u32, c_u32, _P]),
+    "dsplat_point_rasterize_pix_zbuffer_noalloc": (c_i32, [_P, c_u32, _P, _P, _P, _P, _P, c_u32, c_u32]),
     "dsplat_gauss_batch_layout": (c_i32, [c_i64, c_i32, ctypes.POINTER(View), c_i32, c_i32, c_u64,
                                           ctypes.POINTER(BatchLayout)]),
     "dsplat_gauss_batch_forward": (c_i32, [_P, ctypes.POINTER(GaussParams), c_i32, ctypes.POINTER(View), c_i32,

@@ -124,6 +124,18 @@ int dsplat_point_rasterize_pix_zbuffer(dsplat_stream stream, uint32_t num_pnt, c
                                        const float* pnt2rgb, float* pix2rgb, float* pix2unitdepth,
                                        int32_t* pix2winner, uint32_t img_w, uint32_t img_h, uint64_t* zbuf);
 
+/* No counterpart in the reference.  dsplat_point_rasterize_pix_zbuffer for
+ * callers that cannot hand the library device memory (e.g. a plug-in whose
+ * host application owns every GPU allocation, or a loop that must not call
+ * cudaMalloc): no zbuf argument and nothing is allocated; the 64-bit keys live
+ * in a fixed 2^20-entry (8 MiB) array inside the library, so img_w*img_h must
+ * be <= 1048576 (larger images return DSPLAT_ERR_INVALID_ARG).  The first call
+ * on a device looks the array up; make it before any stream capture.  Calls
+ * share the array: calls whose GPU work overlaps race. */
+int dsplat_point_rasterize_pix_zbuffer_noalloc(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxyndcz,
+                                               const float* pnt2rgb, float* pix2rgb, float* pix2unitdepth,
+                                               int32_t* pix2winner, uint32_t img_w, uint32_t img_h);
+
 /* del-splat-dlpack/src/splat_point.rs:12-43 point_splat_rasterize_pix (the
  * reference has only a CPU branch, its GPU arm is todo!()). */
 int dsplat_point_rasterize_pix(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxyndcz,
