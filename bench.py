@@ -182,8 +182,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1 << 20)
     ap.add_argument("--views", type=int, default=16)
-    ap.add_argument("--tile", type=int, default=8)
-    ap.add_argument("--ppl", type=int, default=0, help="rasteriser pixels per lane (0: default)")
+    ap.add_argument("--tile", type=int, default=0, help="tile size 8/16/32; 0: autotune (with --ppl)")
+    ap.add_argument("--ppl", type=int, default=0, help="rasteriser pixels per lane (0: default / autotune)")
+    ap.add_argument("--no-graph", action="store_true", help="time the batched step without CUDA-graph replay")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -212,6 +213,10 @@ def main():
     target = torch.from_numpy(np.concatenate([t.reshape(-1) for t in tgt_np])).to(dev)
     grads = {k: torch.zeros_like(v) for k, v in params.items()}
 
+    tune_report = {}
+    if args.tile == 0:
+        from dsplat import autotune
+        args.tile, args.ppl = autotune.tune(params, cams, 3, target, use_cache=False, report=tune_report)
     batch = GaussBatch(base.n, cams, args.tile, 3, pair_capacity=1 << 24, device=dev, pixels_per_lane=args.ppl)
     pairs = batch.ensure_capacity(params)
     V = len(cams)
@@ -250,7 +255,29 @@ def main():
         step_batched()
     torch.cuda.synchronize()
 
+    # per-stage times (CUDA events on the launch stream) from an instrumented pass
     stage_ms = np.zeros(9)
+    for _ in range(args.steps):
+        L.dsplat_set_stage_events(handles, 10)
+        step_batched()
+        L.dsplat_set_stage_events(None, 0)
+        torch.cuda.synchronize()
+        stage_ms += [evs[i].elapsed_time(evs[i + 1]) for i in range(9)]
+    stage_ms /= args.steps
+
+    graph = None
+    if not args.no_graph:
+        from dsplat.gauss import CapturedStep
+        graph = CapturedStep(batch, params, grads, target)
+        for _ in range(args.warmup):
+            graph.replay()
+        torch.cuda.synchronize()
+    run_batched = graph.replay if graph is not None else step_batched
+
+    c0 = L.dsplat_launch_count()
+    step_batched()
+    torch.cuda.synchronize()
+    per_step_launches = L.dsplat_launch_count() - c0
     n_launch0 = L.dsplat_launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(world)
@@ -258,18 +285,15 @@ def main():
     with ClockSampler(local) as clk:
         e0.record()
         for _ in range(args.steps):
-            L.dsplat_set_stage_events(handles, 10)
-            step_batched()
-            L.dsplat_set_stage_events(None, 0)
-            torch.cuda.synchronize()
-            stage_ms += [evs[i].elapsed_time(evs[i + 1]) for i in range(9)]
+            run_batched()
         e1.record()
         torch.cuda.synchronize()
     barrier(world)
     launches = L.dsplat_launch_count() - n_launch0
+    if graph is not None:  # a replay re-issues the captured launches without calling the library
+        launches = per_step_launches * args.steps
     t_ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
     value = world * V * args.steps / (t_ms / 1e3)
-    stage_ms /= args.steps
     clocks = clk.summary()
 
     # untimed check: no capacity overflow happened
@@ -360,7 +384,8 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG64; no public dataset)",
             "config": {"workload": "1M Gaussians SH3, 16 views mixed 320x240..1920x1080, fwd+bwd, L2 loss",
                        "num_gaussians": base.n, "views_per_gpu": V, "tile_size": args.tile,
-                       "pixels_per_lane": batch.ppl or None,
+                       "pixels_per_lane": batch.ppl or None, "cuda_graph": graph is not None,
+                       "autotune": tune_report or None,
                        "pairs_per_step": int(pairs_now), "pixels_per_step": npix,
                        "plain_views_per_s": plain_vps,
                        "batched_over_plain": (value / world) / (plain_vps / world) if plain_vps else None,

@@ -239,3 +239,34 @@ def adam_step(param: torch.Tensor, grad: torch.Tensor, exp_avg: torch.Tensor, ex
     N.check(N.lib().dsplat_adam_step(_stream_ptr(param.device), param.numel(), param.data_ptr(), grad.data_ptr(),
                                      exp_avg.data_ptr(), exp_avg_sq.data_ptr(), lr, beta1, beta2, eps, step),
             "adam_step")
+
+
+class CapturedStep:
+    """A whole batched training step (zero grads, forward with L2 loss, backward)
+    captured into one CUDA graph.  The batch's forward has no host
+    synchronisation (fixed list capacity, overflow reported by a device flag),
+    so the step replays with zero host work per kernel."""
+
+    def __init__(self, batch: GaussBatch, params: Dict[str, torch.Tensor], grads: Dict[str, torch.Tensor],
+                 target: torch.Tensor, warmup: int = 2):
+        self.batch, self.params, self.grads, self.target = batch, params, grads, target
+        side = torch.cuda.Stream(batch.device)
+        side.wait_stream(torch.cuda.current_stream(batch.device))
+        with torch.cuda.stream(side):
+            for _ in range(warmup):
+                self._step()
+        torch.cuda.current_stream(batch.device).wait_stream(side)
+        torch.cuda.synchronize(batch.device)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._step()
+        torch.cuda.synchronize(batch.device)
+
+    def _step(self):
+        for g in self.grads.values():
+            g.zero_()
+        self.batch.forward(self.params, target=self.target)
+        self.batch.backward(self.params, self.grads)
+
+    def replay(self):
+        self.graph.replay()

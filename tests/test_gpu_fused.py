@@ -96,3 +96,37 @@ def test_empty_scene(dev):
     batch = GaussBatch(0, cams, 16, -1, pair_capacity=16, device=dev)
     img = batch.forward(p)
     assert float(img.abs().max()) == 0.0
+
+
+def test_graph_captured_step_matches_eager(dev):
+    """The whole batched fwd+bwd step captured into a CUDA graph gives the same
+    images and gradients as the eager calls."""
+    from dsplat.gauss import CapturedStep
+    sc = _scene(3, n=8000)
+    p = params_of(sc, dev)
+    batch = GaussBatch(sc.n, sc.cameras, 16, 3, pair_capacity=1000, device=dev, pixels_per_lane=2)
+    batch.ensure_capacity(p)
+    npix = int(batch.layout.num_pix)
+    target = torch.rand(npix * 3, device=dev)
+    grads = {k: torch.zeros_like(v) for k, v in p.items()}
+    batch.forward(p, target=target)
+    batch.backward(p, grads)
+    torch.cuda.synchronize()
+    img_eager = batch.out_rgb.clone()
+    g_eager = {k: v.clone() for k, v in grads.items()}
+    step = CapturedStep(batch, p, grads, target)
+    step.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(batch.out_rgb, img_eager)
+    for k in g_eager:
+        assert torch.allclose(grads[k], g_eager[k], rtol=1e-5, atol=1e-6), k
+
+
+def test_autotuner_picks_a_supported_config(dev):
+    from dsplat import autotune
+    sc = _scene(0, n=4000)
+    p = params_of(sc, dev)
+    npix = sum(c.width * c.height for c in sc.cameras)
+    rep = {}
+    ts, ppl = autotune.tune(p, sc.cameras, 0, torch.rand(npix * 3, device=dev), use_cache=False, report=rep)
+    assert (ts, ppl) in autotune.CANDIDATES and len(rep["timings_ms"]) == len(autotune.CANDIDATES)
