@@ -149,7 +149,7 @@ int build_sb_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npa
   const size_t m = size_t(b.num_sb) * nchunk;
   const unsigned grid1 = unsigned(b.num_views) * nchunk;
   const size_t smem1 = size_t(b.max_sb) * sizeof(uint32_t);
-  const size_t smem3 = 8 * smem1;
+  const size_t smem3 = 8 * smem1 + 8 * 512 * sizeof(uint32_t);
   if (smem3 > 48 * 1024) {
     if (smem3 > 200 * 1024) return fail(DSPLAT_ERR_UNSUPPORTED, "too many superblocks in one view");
     TRY_CUDA(cudaFuncSetAttribute(k_sb_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)), "attr");

@@ -333,36 +333,27 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restr
 
 // ---------------------------------------------------------------------------
 // Stage 1b: stable scatter of point indices into superblock lists.  Warp w
-// owns ranks [w*512, w*512+512) of the chunk in 16 rounds of 32; inside a
-// round a lane's rank among the lanes that hit the same superblock is counted
-// from the other lanes' spans (fetched by shuffle).
+// owns ranks [w*512, w*512+512) of the chunk in 16 rounds of 32.  In a round,
+// one ballot per superblock column and per superblock row of the view says
+// which lanes' spans cover it; the lanes covering superblock (x, y) are then
+// colmask[x] & rowmask[y], and a lane's slot is its popcount among them.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void lane_rank(const uint32_t* spans, int lane, int sx, int sy, int* below, int* above) {
-  int bl = 0, ab = 0;
-#pragma unroll
-  for (int l = 0; l < 32; ++l) {
-    const uint32_t p = spans[l];
-    const int ax0 = p & 255, ay0 = (p >> 8) & 255, ax1 = (p >> 16) & 255, ay1 = p >> 24;
-    const bool in = sx >= ax0 && sx < ax1 && sy >= ay0 && sy < ay1;
-    bl += (in && l < lane);
-    ab += (in && l > lane);
-  }
-  *below = bl;
-  *above = ab;
-}
-
 __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __restrict__ order,
                                                            const uint2* __restrict__ rect, uint32_t n, uint32_t npad,
                                                            const ViewBatch b,
                                                            const uint32_t* __restrict__ off, uint64_t capacity,
                                                            uint2* __restrict__ list1, uint32_t* __restrict__ flags) {
-  extern __shared__ uint32_t wc[];  // [kMsWarps][nsb]
+  extern __shared__ uint32_t smem_ms[];  // [kMsWarps][nsb] counters, then [kMsWarps][256+256] masks
   const uint32_t nchunk = npad / kMsChunk;
   const uint32_t v = blockIdx.x / nchunk, c = blockIdx.x % nchunk;
   const ViewDev& vd = b.v[v];
   const int sbw = (vd.tile_w + 7) >> 3, sbh = (vd.tile_h + 7) >> 3;
   const int nsb = sbw * sbh;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t* wc = smem_ms;
+  uint32_t* colmask = smem_ms + kMsWarps * b.max_sb + warp * 512;
+  uint32_t* rowmask = colmask + 256;
   for (int i = threadIdx.x; i < kMsWarps * nsb; i += kMsThreads) wc[i] = 0;
   __syncthreads();
   const size_t base = size_t(v) * npad + size_t(c) * kMsChunk + size_t(warp) * (kMsRounds * 32);
@@ -388,32 +379,47 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
   }
   __syncthreads();
   // phase 3: stable scatter, round by round
-  uint32_t spans[32];
   for (int r = 0; r < kMsRounds; ++r) {
     const uint32_t g = order[base + r * 32 + lane];
     int sx0 = 0, sy0 = 0, sx1 = 0, sy1 = 0;
     const uint2 rc = g < n ? rect[size_t(v) * n + g] : make_uint2(0u, 0u);
     const bool has = g < n && sb_span(rc, &sx0, &sy0, &sx1, &sy1);
-    const uint32_t packed =
-        has ? (uint32_t(sx0) | uint32_t(sy0) << 8 | uint32_t(sx1) << 16 | uint32_t(sy1) << 24) : 0u;
+    // the round's column / row coverage masks
+    int cx0 = has ? sx0 : 255, cx1 = has ? sx1 : 0, cy0 = has ? sy0 : 255, cy1 = has ? sy1 : 0;
 #pragma unroll
-    for (int l = 0; l < 32; ++l) spans[l] = __shfl_sync(0xffffffffu, packed, l);
-    for (int sy = sy0; sy < sy1; ++sy)
+    for (int o = 16; o > 0; o >>= 1) {
+      cx0 = min(cx0, __shfl_xor_sync(0xffffffffu, cx0, o));
+      cx1 = max(cx1, __shfl_xor_sync(0xffffffffu, cx1, o));
+      cy0 = min(cy0, __shfl_xor_sync(0xffffffffu, cy0, o));
+      cy1 = max(cy1, __shfl_xor_sync(0xffffffffu, cy1, o));
+    }
+    for (int x = cx0; x < cx1; ++x) {
+      const uint32_t m = __ballot_sync(0xffffffffu, has && x >= sx0 && x < sx1);
+      if (lane == 0) colmask[x] = m;
+    }
+    for (int y = cy0; y < cy1; ++y) {
+      const uint32_t m = __ballot_sync(0xffffffffu, has && y >= sy0 && y < sy1);
+      if (lane == 0) rowmask[y] = m;
+    }
+    __syncwarp();
+    for (int sy = sy0; sy < sy1; ++sy) {
+      const uint32_t rm = rowmask[sy];
       for (int sx = sx0; sx < sx1; ++sx) {
-        int below, above;
-        lane_rank(spans, lane, sx, sy, &below, &above);
-        const uint32_t dst = my[sy * sbw + sx] + uint32_t(below);
+        const uint32_t m = colmask[sx] & rm;
+        const uint32_t dst = my[sy * sbw + sx] + uint32_t(__popc(m & lt));
         if (dst < capacity) list1[dst] = make_uint2(g, local_rect(rc, sx, sy));
         else set_flag(flags, kFlagPairOverflow);
       }
+    }
     __syncwarp();
-    // the highest lane hitting a superblock advances the warp's counter
-    for (int sy = sy0; sy < sy1; ++sy)
+    // the highest lane covering a superblock advances the warp's counter
+    for (int sy = sy0; sy < sy1; ++sy) {
+      const uint32_t rm = rowmask[sy];
       for (int sx = sx0; sx < sx1; ++sx) {
-        int below, above;
-        lane_rank(spans, lane, sx, sy, &below, &above);
-        if (above == 0) my[sy * sbw + sx] += uint32_t(below + 1);
+        const uint32_t m = colmask[sx] & rm;
+        if ((m >> lane) == 1u) my[sy * sbw + sx] += uint32_t(__popc(m));
       }
+    }
     __syncwarp();
   }
 }

@@ -118,8 +118,9 @@ def test_graph_captured_step_matches_eager(dev):
     step.replay()
     torch.cuda.synchronize()
     assert torch.equal(batch.out_rgb, img_eager)
-    for k in g_eager:
-        assert torch.allclose(grads[k], g_eager[k], rtol=1e-5, atol=1e-6), k
+    for k in g_eager:  # float atomics may add in another order: compare at the group's scale
+        scale = g_eager[k].abs().max()
+        assert (grads[k] - g_eager[k]).abs().max() <= 1e-4 * scale, k
 
 
 def test_autotuner_picks_a_supported_config(dev):
