@@ -47,9 +47,9 @@ cudaError_t raster_bwd(cudaStream_t, const ViewBatch&, const BwdArgs&);
 bool raster_config_ok(int ts, int ppl);
 int raster_default_ppl(int ts);
 uint32_t raster_slabs_per_tile(int ts, int ppl);
-__global__ void k_order_hist(const ViewBatch, const uint32_t*, uint32_t, uint32_t*);
+__global__ void k_order_hist(const ViewBatch, const uint32_t*, uint32_t, const uint32_t*, uint32_t*);
 __global__ void k_order_scan(uint32_t*);
-__global__ void k_order_scatter(const ViewBatch, const uint32_t*, uint32_t, uint32_t*, uint32_t*);
+__global__ void k_order_scatter(const ViewBatch, const uint32_t*, uint32_t, const uint32_t*, uint32_t*, uint32_t*);
 cudaError_t raster_fwd_aos(cudaStream_t, int, int, int, float*, const float*, const float*, const float*, const float*,
                            const float*, const uint32_t*, const uint32_t*, float*, uint32_t*);
 cudaError_t circle_splat_tiles(cudaStream_t, int, int, int, float*, const float*, const float*, const float*,
@@ -182,6 +182,19 @@ int build_tile_lists(cudaStream_t st, const ViewBatch& b, uint32_t npad, const L
   count_launch();
   TRY_CUDA(cudaGetLastError(), "tile lists");
   return DSPLAT_OK;
+}
+
+cudaError_t order_tasks(cudaStream_t st, const ViewBatch& b, const uint32_t* off1, uint32_t nchunk,
+                        const uint32_t* cost, uint32_t* sched, uint32_t* order) {
+  cudaError_t e = cudaMemsetAsync(sched, 0, 80 * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
+  k_order_hist<<<64, 256, 0, st>>>(b, off1, nchunk, cost, sched);
+  count_launch();
+  k_order_scan<<<1, 32, 0, st>>>(sched);
+  count_launch();
+  k_order_scatter<<<64, 256, 0, st>>>(b, off1, nchunk, cost, sched, order);
+  count_launch();
+  return cudaGetLastError();
 }
 
 void fill_sb_layout(ViewBatch* b) {
@@ -327,7 +340,7 @@ struct BatchWs {
   float* grad_pix;
   float* slab_loss;
   float4* grad2d;
-  uint32_t *sched, *task_order;
+  uint32_t *sched, *task_order, *task_order_bwd, *item_cost;
 };
 
 int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, int32_t ppl, ViewBatch* b) {
@@ -404,6 +417,8 @@ BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity)
   w.grad2d = c.take<float4>(3 * VN + 3, &L.off_grad2d);
   w.sched = c.take<uint32_t>(80);
   w.task_order = c.take<uint32_t>(size_t(b.num_items) + 1);
+  w.task_order_bwd = c.take<uint32_t>(size_t(b.num_items) + 1);
+  w.item_cost = c.take<uint32_t>(size_t(b.num_items) + 1);
   L.total_bytes = align_up(c.off, 256);
   return w;
 }
@@ -623,17 +638,13 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
     if (rc2) return rc2;
     stage_mark(st, 3);
   }
-  // longest-first raster task order
-  TRY_CUDA(cudaMemsetAsync(w.sched, 0, 80 * sizeof(uint32_t), st), "memset");
-  k_order_hist<<<64, 256, 0, st>>>(b, w.lists.off1, npad / kChunk, w.sched);
-  count_launch();
-  k_order_scan<<<1, 32, 0, st>>>(w.sched);
-  count_launch();
-  k_order_scatter<<<64, 256, 0, st>>>(b, w.lists.off1, npad / kChunk, w.sched, w.task_order);
-  count_launch();
+  // longest-first raster task order (costs measured by the previous forward)
+  TRY_CUDA(order_tasks(st, b, w.lists.off1, npad / kChunk, w.item_cost, w.sched, w.task_order), "task order");
+  TRY_CUDA(cudaMemsetAsync(w.item_cost, 0, size_t(b.num_items) * sizeof(uint32_t), st), "memset");
   stage_mark(st, 4);
-  const FwdArgs fa{n,        w.rec,        w.lists.list1, w.lists.off1, npad / kChunk, pair_capacity, w.task_order,
-                   w.flags + 2, out_rgb, w.pix_T,        w.pix_stop,   target,        w.grad_pix,    w.slab_loss};
+  const FwdArgs fa{n,           w.rec,   w.lists.list1, w.lists.off1, npad / kChunk, pair_capacity, w.task_order,
+                   w.flags + 2, out_rgb, w.pix_T,       w.pix_stop,   target,        w.grad_pix,    w.slab_loss,
+                   w.item_cost};
   TRY_CUDA(raster_fwd(st, b, fa),
            "raster_fwd");
   stage_mark(st, 5);
@@ -667,9 +678,11 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
   stage_mark(st, 6);
   TRY_CUDA(cudaMemsetAsync(w.grad2d, 0, 3 * VN * sizeof(float4), st), "memset");
   TRY_CUDA(cudaMemsetAsync(w.flags + 3, 0, sizeof(uint32_t), st), "memset");
+  // longest-first order from this forward's measured walks
+  TRY_CUDA(order_tasks(st, b, w.lists.off1, w.L.npad / kChunk, w.item_cost, w.sched, w.task_order_bwd), "task order");
   stage_mark(st, 7);
   const BwdArgs ba{n,           w.rec,    w.lists.list1,  w.lists.off1, w.L.npad / kChunk, pair_capacity,
-                   w.task_order, w.flags + 3, grad_rgb ? grad_rgb : w.grad_pix, w.pix_T, w.pix_stop, w.grad2d};
+                   w.task_order_bwd, w.flags + 3, grad_rgb ? grad_rgb : w.grad_pix, w.pix_T, w.pix_stop, w.grad2d};
   TRY_CUDA(raster_bwd(st, b, ba),
            "raster_bwd");
   stage_mark(st, 8);

@@ -56,6 +56,7 @@ struct FwdArgs {
   const float* target;
   float* grad_pix;
   float* slab_loss;
+  uint32_t* item_cost;
 };
 
 struct BwdArgs {

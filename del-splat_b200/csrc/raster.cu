@@ -132,7 +132,7 @@ __device__ __forceinline__ float quad(float B, float C, float dx, float dy, floa
 // of the time.
 // ---------------------------------------------------------------------------
 template <int TS, int PPL_, class Walk, class Src>
-__device__ __forceinline__ void fwd_slab(const Walk& walk, const Src& src, Ent* sm, uint32_t s, uint32_t e, int px0,
+__device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, Ent* sm, uint32_t s, uint32_t e, int px0,
                                          int py0, int w, int h, bool accumulate, float* __restrict__ out_rgb,
                                          size_t pix_base, float* __restrict__ out_T, uint32_t* __restrict__ out_last,
                                          const float* __restrict__ target, float* __restrict__ grad_pix,
@@ -164,7 +164,8 @@ __device__ __forceinline__ void fwd_slab(const Walk& walk, const Src& src, Ent* 
     }
   }
   const uint32_t inside = live;
-  for (uint32_t hi = e; hi > s;) {
+  uint32_t hi = e;
+  while (hi > s) {
     const int cnt = int(min(32u, hi - s));
     const int k_staged = walk.stage(src, sm, hi - 1u - uint32_t(lane), lane < cnt, lane);
     __syncwarp();
@@ -226,6 +227,7 @@ __device__ __forceinline__ void fwd_slab(const Walk& walk, const Src& src, Ent* 
     for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
     if (lane == 0) *loss_slot = l;
   }
+  return e - hi;
 }
 
 // The superblock-list range of an item and the tile's place in it.
@@ -263,7 +265,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     const uint32_t* __restrict__ off1, uint32_t nchunk, uint64_t capacity, const uint32_t* __restrict__ order,
     uint32_t* __restrict__ work_counter, float* __restrict__ out_rgb, float* __restrict__ out_T,
     uint32_t* __restrict__ out_last, const float* __restrict__ target, float* __restrict__ grad_pix,
-    float* __restrict__ slab_loss) {
+    float* __restrict__ slab_loss, uint32_t* __restrict__ item_cost) {
   using G = Geo<TS, PPL>;
   __shared__ Ent sm_all[kRasterWarps][32];
   Ent* sm = sm_all[threadIdx.x >> 5];
@@ -279,9 +281,12 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     const ViewDev& vd = b.v[ig.v];
     PackedSrc src{rec + 3 * size_t(ig.v) * n};
     SbWalk walk{list1, ig.lx, ig.ly};
-    fwd_slab<TS, PPL>(walk, src, sm, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, false,
-                      out_rgb, vd.pix_base, out_T, out_last, target, grad_pix,
-                      slab_loss ? slab_loss + size_t(item) * G::SLABS + slab : nullptr);
+    const uint32_t walked =
+        fwd_slab<TS, PPL>(walk, src, sm, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, false,
+                          out_rgb, vd.pix_base, out_T, out_last, target, grad_pix,
+                          slab_loss ? slab_loss + size_t(item) * G::SLABS + slab : nullptr);
+    // scheduling hint for the backward and the next forward: list positions walked
+    if (lane == 0 && walked) atomicMax(&item_cost[item], walked);
     __syncwarp();
   }
 }
@@ -492,7 +497,7 @@ static int num_sms() {
 
 // Supported (tile size, pixels per lane) pairs; slabs per tile follow.
 bool raster_config_ok(int ts, int ppl) {
-  return (ts == 8 && ppl == 2) || (ts == 16 && (ppl == 2 || ppl == 4 || ppl == 8)) ||
+  return (ts == 8 && (ppl == 1 || ppl == 2)) || (ts == 16 && (ppl == 2 || ppl == 4 || ppl == 8)) ||
          (ts == 32 && (ppl == 4 || ppl == 8));
 }
 int raster_default_ppl(int ts) { return ts == 8 ? 2 : 4; }
@@ -514,7 +519,7 @@ static void launch_fwd(cudaStream_t st, const ViewBatch& b, const FwdArgs& a) {
   const uint32_t tasks = b.num_items * Geo<TS, PPL>::SLABS;
   k_raster_fwd<TS, PPL><<<persistent_grid(k_raster_fwd<TS, PPL>, tasks), 32 * kRasterWarps, 0, st>>>(
       b, a.n, a.rec, a.list1, a.off1, a.nchunk, a.capacity, a.order, a.counter, a.out_rgb, a.out_T, a.out_last,
-      a.target, a.grad_pix, a.slab_loss);
+      a.target, a.grad_pix, a.slab_loss, a.item_cost);
   count_launch();
 }
 
@@ -527,7 +532,7 @@ static void launch_bwd(cudaStream_t st, const ViewBatch& b, const BwdArgs& a) {
   count_launch();
 }
 
-#define DSPLAT_RASTER_CONFIGS(X) X(8, 2) X(16, 2) X(16, 4) X(16, 8) X(32, 4) X(32, 8)
+#define DSPLAT_RASTER_CONFIGS(X) X(8, 1) X(8, 2) X(16, 2) X(16, 4) X(16, 8) X(32, 4) X(32, 8)
 
 cudaError_t raster_fwd(cudaStream_t st, const ViewBatch& b, const FwdArgs& a) {
 #define X(T, P)                        \

@@ -543,12 +543,16 @@ __global__ void __launch_bounds__(kMsThreads) k_tile_scatter(const uint2* __rest
 
 // ---------------------------------------------------------------------------
 // Longest-first task order for the rasteriser: items bucketed by floor(log2)
-// of their superblock-list length, heaviest bucket first, so the tail of the
-// persistent launch is made of short tasks.  sched[0..31] counts, [32..63]
-// cursors.
+// of their cost, heaviest bucket first, so the tail of the persistent launch
+// is made of short tasks.  The cost is the number of list positions the last
+// forward walked for the item (measured, kept in the workspace) or, where
+// none is recorded yet, its superblock-list length.  Only the schedule
+// depends on it, never the results.  sched[0..32] counts, [40..72] cursors.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t item_cost_bucket(const ViewBatch& b, uint32_t item, const uint32_t* off1,
-                                                     uint32_t nchunk) {
+                                                     uint32_t nchunk, const uint32_t* cost) {
+  const uint32_t measured = cost ? cost[item] : 0u;
+  if (measured) return uint32_t(__clz(measured));
   int v = 0;
   for (int k = 1; k < b.num_views; ++k)
     if (item >= b.v[k].item_base) v = k;
@@ -561,12 +565,12 @@ __device__ __forceinline__ uint32_t item_cost_bucket(const ViewBatch& b, uint32_
 }
 
 __global__ void k_order_hist(const ViewBatch b, const uint32_t* __restrict__ off1, uint32_t nchunk,
-                             uint32_t* __restrict__ sched) {
+                             const uint32_t* __restrict__ cost, uint32_t* __restrict__ sched) {
   __shared__ uint32_t h[33];
   if (threadIdx.x < 33) h[threadIdx.x] = 0;
   __syncthreads();
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.num_items; i += gridDim.x * blockDim.x)
-    atomicAdd(&h[item_cost_bucket(b, i, off1, nchunk)], 1u);
+    atomicAdd(&h[item_cost_bucket(b, i, off1, nchunk, cost)], 1u);
   __syncthreads();
   if (threadIdx.x < 33 && h[threadIdx.x]) atomicAdd(&sched[threadIdx.x], h[threadIdx.x]);
 }
@@ -582,9 +586,10 @@ __global__ void k_order_scan(uint32_t* __restrict__ sched) {
 }
 
 __global__ void k_order_scatter(const ViewBatch b, const uint32_t* __restrict__ off1, uint32_t nchunk,
-                                uint32_t* __restrict__ sched, uint32_t* __restrict__ order) {
+                                const uint32_t* __restrict__ cost, uint32_t* __restrict__ sched,
+                                uint32_t* __restrict__ order) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.num_items; i += gridDim.x * blockDim.x)
-    order[atomicAdd(&sched[40 + item_cost_bucket(b, i, off1, nchunk)], 1u)] = i;
+    order[atomicAdd(&sched[40 + item_cost_bucket(b, i, off1, nchunk, cost)], 1u)] = i;
 }
 
 // Clamp tile ranges to the pair capacity after an overflow so that readers

@@ -16,7 +16,7 @@ import torch
 from .gauss import GaussBatch
 from .scenes import Camera
 
-CANDIDATES: Tuple[Tuple[int, int], ...] = ((8, 2), (16, 2), (16, 4), (32, 4))
+CANDIDATES: Tuple[Tuple[int, int], ...] = ((8, 1), (8, 2), (16, 2), (16, 4), (32, 4))
 _memo: Dict[str, Tuple[int, int]] = {}
 
 

@@ -53,7 +53,7 @@ def _check_view(orc, batch, sc, v, ts):
     assert np.array_equal(stop, o_last)
 
 
-@pytest.mark.parametrize("sh_deg,ts,ppl", [(-1, 16, 0), (0, 16, 2), (1, 8, 2), (3, 16, 4), (3, 16, 8), (3, 32, 4),
+@pytest.mark.parametrize("sh_deg,ts,ppl", [(-1, 16, 0), (0, 16, 2), (1, 8, 2), (3, 8, 1), (3, 16, 4), (3, 16, 8), (3, 32, 4),
                                             (2, 32, 8)])
 def test_batched_forward_matches_oracle(orc, dev, sh_deg, ts, ppl):
     sc = _scene(sh_deg)
