@@ -131,8 +131,6 @@ __device__ __forceinline__ float quad(float B, float C, float dx, float dy, floa
 // (pixel done, row outside the entry's box) are uniform across the warp most
 // of the time.
 // ---------------------------------------------------------------------------
-constexpr int kGroup = 8;  // list entries whose alphas are evaluated together
-
 template <int TS, int PPL_, class Walk, class Src>
 __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, Ent* sm, uint32_t s, uint32_t e, int px0,
                                          int py0, int w, int h, bool accumulate, float* __restrict__ out_rgb,
@@ -171,49 +169,34 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
     const int cnt = int(min(32u, hi - s));
     const int k_staged = walk.stage(src, sm, hi - 1u - uint32_t(lane), lane < cnt, lane);
     __syncwarp();
-    // Groups of kGroup entries: the alphas of every (entry, pixel slot) pair of
-    // the group are computed first -- independent exps, so even a warp running
-    // alone issues back to back -- then blended in list order.  A slot outside
-    // an entry's box, or already done, gets alpha 0, which leaves colour, T and
-    // alpha_sum bit-for-bit unchanged (x*0 = +-0, y + +-0 = y).
-    for (int j0 = 0; live && j0 < k_staged; j0 += kGroup) {
-      float al[kGroup][PPL];
-#pragma unroll
-      for (int jj = 0; jj < kGroup; ++jj) {
-        const int j = j0 + jj;
+    if (live) {
+      for (int j = 0; j < k_staged; ++j) {
         const float4 ea = sm[j].a, eb = sm[j].b, ec = sm[j].c, ed = sm[j].d;
-        const bool xin = j < k_staged && ec.y <= fx && fx <= ec.w;
+        if (!(ec.y <= fx && fx <= ec.w)) continue;
         const float dx = fs(fx, ea.x);
         const float adxdx = fm(fm(ea.z, dx), dx);
-#pragma unroll
-        for (int k = 0; k < PPL; ++k) {
-          const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
-          const bool in = xin && ((live >> k) & 1u) && ec.z <= fy && fy <= ed.x;
-          const float dy = fs(fy, ea.y);
-          const float q = quad(ea.w, eb.x, dx, dy, adxdx);
-          const float a = fm(dexp(fm(-0.5f, q)), eb.y);
-          al[jj][k] = in ? a : 0.f;
-        }
-      }
-#pragma unroll
-      for (int jj = 0; jj < kGroup; ++jj) {
-        const int j = min(j0 + jj, k_staged - 1);
-        const float4 eb = sm[j].b, ec = sm[j].c, ed = sm[j].d;
         const uint32_t pos = __float_as_uint(ed.z);
 #pragma unroll
         for (int k = 0; k < PPL; ++k) {
+          // a slot is one row pair across the warp: the skip is warp-uniform in practice
           if (!((live >> k) & 1u)) continue;
-          const float eo = fm(T[k], al[jj][k]);
+          const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
+          if (!(ec.z <= fy && fy <= ed.x)) continue;
+          const float dy = fs(fy, ea.y);
+          const float q = quad(ea.w, eb.x, dx, dy, adxdx);
+          const float al = fm(dexp(fm(-0.5f, q)), eb.y);
+          const float eo = fm(T[k], al);
           c0[k] = fa(c0[k], fm(eb.z, eo));
           c1[k] = fa(c1[k], fm(eb.w, eo));
           c2[k] = fa(c2[k], fm(ec.x, eo));
-          T[k] = fm(T[k], fs(1.f, al[jj][k]));
+          T[k] = fm(T[k], fs(1.f, al));
           as[k] = fa(as[k], eo);
           if (as[k] >= kAlphaBreak) {
             live &= ~(1u << k);
             last[k] = pos;
           }
         }
+        if (!live) break;
       }
     }
     hi -= uint32_t(cnt);
