@@ -197,12 +197,36 @@ cudaError_t order_tasks(cudaStream_t st, const ViewBatch& b, const uint32_t* off
   return cudaGetLastError();
 }
 
+// Superblock side per view.  A tile walks its whole superblock list when its
+// pixels never saturate (silhouettes, sparse regions), so the list length,
+// ~ visible points x superblock area / view area, bounds the slowest raster
+// task; stage 1 instead pays per superblock a point spans.  Rule: the
+// largest side (8 tiles at most) that still splits the view into at least
+// kSbMinPerView superblocks -- a fixed fraction of the view -- within the
+// per-view limits of the stage-1 kernels (255 per side, kSbMaxPerView).
+constexpr uint32_t kSbMinPerView = 200;
+constexpr uint32_t kSbMaxPerView = 4096;
+
+int choose_sb_log2(int tile_w, int tile_h) {
+  int s = 3;
+  while (s > 0) {
+    const uint32_t cw = uint32_t((tile_w + (1 << s) - 1) >> s), ch = uint32_t((tile_h + (1 << s) - 1) >> s);
+    if (cw * ch >= kSbMinPerView) break;
+    const uint32_t nw = uint32_t((tile_w + (1 << (s - 1)) - 1) >> (s - 1));
+    const uint32_t nh = uint32_t((tile_h + (1 << (s - 1)) - 1) >> (s - 1));
+    if (nw > 255 || nh > 255 || nw * nh > kSbMaxPerView) break;
+    --s;
+  }
+  return s;
+}
+
 void fill_sb_layout(ViewBatch* b) {
   uint32_t sb = 0, mx = 0;
   for (int v = 0; v < b->num_views; ++v) {
     ViewDev& d = b->v[v];
     d.sb_base = sb;
-    const uint32_t c = uint32_t((d.tile_w + 7) / 8) * uint32_t((d.tile_h + 7) / 8);
+    d.sb_log2 = choose_sb_log2(d.tile_w, d.tile_h);
+    const uint32_t c = uint32_t(sb_cols(d)) * uint32_t(sb_rows(d));
     sb += c;
     mx = c > mx ? c : mx;
   }
@@ -410,6 +434,7 @@ BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity)
   carve_lists(c, b, npad, cap, &w.lists, &L.off_sb_list, &L.off_sb_start);
   L.sb_chunks = npad / kChunk;
   L.num_sb = b.num_sb;
+  for (int v = 0; v < b.num_views; ++v) L.sb_log2[v] = b.v[v].sb_log2;
   w.pix_T = c.take<float>(b.num_pix, &L.off_pix_T);
   w.pix_stop = c.take<uint32_t>(b.num_pix, &L.off_pix_stop);
   w.grad_pix = c.take<float>(size_t(b.num_pix) * 3, &L.off_grad_pix);

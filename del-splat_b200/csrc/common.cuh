@@ -25,8 +25,17 @@ struct ViewDev {
   int32_t tile_w, tile_h;
   uint32_t item_base;  // first global (view, tile) item of this view
   uint32_t pix_base;   // first pixel of this view in the concatenated images
-  uint32_t sb_base;    // first superblock (8x8 tiles) of this view
+  uint32_t sb_base;    // first superblock of this view
+  int32_t sb_log2;     // superblock side = 1 << sb_log2 tiles (0..3)
 };
+
+// superblock grid of a view
+__host__ __device__ __forceinline__ int sb_cols(const ViewDev& d) {
+  return (d.tile_w + (1 << d.sb_log2) - 1) >> d.sb_log2;
+}
+__host__ __device__ __forceinline__ int sb_rows(const ViewDev& d) {
+  return (d.tile_h + (1 << d.sb_log2) - 1) >> d.sb_log2;
+}
 
 struct ViewBatch {
   int32_t num_views;
@@ -117,6 +126,55 @@ __device__ __forceinline__ float dexp(float x) {
   const int ni = (int)n;
   if (ni < -126) return 0.0f;
   return fm(p, __int_as_float((ni + 127) << 23));
+}
+
+// Fused multiply-add with a single rounding (IEEE fma; the CPU oracle's
+// std::fma gives the same bits).
+__device__ __forceinline__ float ff(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// The rasterisers evaluate exp(-q/2) as 2^y with y = q * (-log2(e)/2); the
+// factor is folded into the staged conic, so y comes out of the quadratic
+// form directly.
+constexpr float kNegHalfLog2e = -0.72134752044448170368f;
+constexpr float kInvNegHalfLog2e = -1.38629436111989061883f;  // -2 ln 2
+
+// Deterministic 2^y: y = n + f with n = nearest integer (the 1.5 * 2^23
+// addition rounds y in the binade where the float spacing is 1; n is read
+// back from the sum's bits), |f| <= 1/2, then the degree-6 Taylor polynomial
+// of e^(f ln 2) (truncation error < 1.2e-7 relative) in Horner form with
+// fused multiply-adds, and the exact scaling by 2^n through the exponent
+// field.  Every step is an exactly rounded IEEE operation, so the CPU oracle
+// reproduces the result bit for bit.  Outside (-125, 123): 0 below, +inf
+// above, NaN stays NaN.
+__device__ __forceinline__ float exp2_det(float y) {
+  if (!(fabsf(__fadd_rn(y, 1.f)) < 124.f)) {
+    if (y != y) return y;
+    return y < 0.f ? 0.f : __int_as_float(0x7f800000);
+  }
+  const float t = __fadd_rn(y, 12582912.f);
+  const float f = __fsub_rn(y, __fsub_rn(t, 12582912.f));
+  float p = 1.5403530393381608e-4f;   // (ln 2)^6 / 720
+  p = ff(p, f, 1.3333558146428443e-3f);  // (ln 2)^5 / 120
+  p = ff(p, f, 9.6181291076284772e-3f);  // (ln 2)^4 / 24
+  p = ff(p, f, 5.5504108664821580e-2f);  // (ln 2)^3 / 6
+  p = ff(p, f, 2.4022650695910071e-1f);  // (ln 2)^2 / 2
+  p = ff(p, f, 6.9314718055994531e-1f);  // ln 2
+  p = ff(p, f, 1.f);
+  const uint32_t n = uint32_t(__float_as_int(t) - __float_as_int(12582912.f));
+  return __int_as_float(int(uint32_t(__float_as_int(p)) + (n << 23)));
+}
+
+// Hardware approximations (PTX ex2.approx / rcp.approx, flush-to-zero) for
+// the backward, whose values need not reproduce the forward bit for bit.
+__device__ __forceinline__ float ex2_approx(float y) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
+  return r;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
 }
 
 // splat_gauss.cu:105 `alpha_sum > 0.999` is a double comparison; for a float

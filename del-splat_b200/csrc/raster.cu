@@ -13,24 +13,31 @@
 // (one coalesced index load + one 48-byte record gather per lane), then every
 // lane walks them with 128-bit broadcast reads, amortising each read over its
 // pixels.  The fused path reads each tile's entries straight out of its
-// superblock list (8x8 tiles, see tiles.cu): a ballot over the 32 fetched
+// superblock list (1-8 tiles per side, see tiles.cu): a ballot over the 32 fetched
 // entries keeps those whose tile span covers the tile, compacted in order, so
 // no per-tile list is ever materialised.  The warp stops fetching as soon as all its pixels terminated
 // (__any_sync), so no CTA-wide barrier exists anywhere.  Warps pull tasks
 // from a global counter (work stealing): one persistent launch covers views
 // of different resolutions.
 //
-// The blend arithmetic uses non-contracted IEEE operations and dexp() so the
-// oracle reproduces it exactly, including every early-exit decision.
+// The blend arithmetic is a fixed sequence of exactly rounded IEEE
+// operations (multiply, add, fused multiply-add) with exp(-q/2) evaluated by
+// exp2_det(); the oracle performs the same sequence, so images, final
+// transmittances and every early-exit decision agree bit for bit.  Versus the
+// reference's expression order the per-pixel values differ only in rounding:
+// y = k q is evaluated as (kA dx) dx + (k2B dx + kC dy) dy, colours
+// accumulate with fma, and T <- T - T alpha replaces T <- T (1 - alpha).
 //
 // Backward (no reference counterpart): the same walk in reverse
 // (back-to-front) from the saved stop position up to the list end; the
 // transmittance in front of each entry is rebuilt from the saved final value,
 // T_i = T_{i+1} / (1 - e_i), and the colour behind it is accumulated, so no
 // per-pixel list is stored.  Each lane sums its pixels' contributions in
-// registers, the warp sums them with shuffles (once per entry for 256
-// pixels) and one lane adds them to the per-(view, point) 2D gradient with
-// vectorised float4 atomics.
+// registers as moments of w = dL/dq (sum w, sum w dy, sum w dy^2 -- dx is
+// fixed per lane), the warp reduces the nine per-entry sums with a
+// transposed butterfly (9 + 5 shuffles instead of 45), and nine lanes add
+// the finished 2D gradient to the per-(view, point) record with one atomic
+// instruction.
 #include "common.cuh"
 
 namespace dsplat {
@@ -38,11 +45,16 @@ namespace dsplat {
 constexpr int kRasterWarps = 4;  // warps per CTA (independent tasks)
 
 struct Ent {  // one staged list entry (64 bytes)
-  float4 a;   // px, py, conic A, conic B
-  float4 b;   // conic C, opacity, r, g
+  float4 a;   // px, py, k A, k 2B   (k = -log2(e)/2: exp(-q/2) = 2^(k q))
+  float4 b;   // k C, opacity, r, g
   float4 c;   // b, box x0, box y0, box x1
-  float4 d;   // box y1, point index (bits), -, -
+  float4 d;   // box y1, point index (bits), list position (bits), -
 };
+
+// The staged conic, scaled so that y = k q = kA dx^2 + (k2B dx + kC dy) dy.
+__device__ __forceinline__ float4 scaled_conic_a(float px, float py, float A, float B) {
+  return make_float4(px, py, fm(A, kNegHalfLog2e), fm(fa(B, B), kNegHalfLog2e));
+}
 
 template <int TS, int PPL_>
 struct Geo {
@@ -57,8 +69,8 @@ __device__ __forceinline__ void stage_packed(Ent* dst, const float4* __restrict_
   const float4 r0 = __ldg(rec + 3 * size_t(g));
   const float4 r1 = __ldg(rec + 3 * size_t(g) + 1);
   const float4 r2 = __ldg(rec + 3 * size_t(g) + 2);
-  dst->a = r0;
-  dst->b = r1;
+  dst->a = scaled_conic_a(r0.x, r0.y, r0.z, r0.w);
+  dst->b = make_float4(fm(r1.x, kNegHalfLog2e), r1.y, r1.z, r1.w);
   dst->c = make_float4(r2.x, fs(r0.x, r2.y), fs(r0.y, r2.z), fa(r0.x, r2.y));
   dst->d = make_float4(fa(r0.y, r2.z), __uint_as_float(g), 0.f, 0.f);
 }
@@ -67,8 +79,8 @@ struct AosSrc {
   const float *xyd, *conic, *aabb, *opacity, *rgb;
   __device__ __forceinline__ void stage(Ent* dst, uint32_t g) const {
     const size_t i = g;
-    dst->a = make_float4(xyd[3 * i], xyd[3 * i + 1], conic[3 * i], conic[3 * i + 1]);
-    dst->b = make_float4(conic[3 * i + 2], opacity[i], rgb[3 * i], rgb[3 * i + 1]);
+    dst->a = scaled_conic_a(xyd[3 * i], xyd[3 * i + 1], conic[3 * i], conic[3 * i + 1]);
+    dst->b = make_float4(fm(conic[3 * i + 2], kNegHalfLog2e), opacity[i], rgb[3 * i], rgb[3 * i + 1]);
     dst->c = make_float4(rgb[3 * i + 2], aabb[4 * i], aabb[4 * i + 1], aabb[4 * i + 2]);
     dst->d = make_float4(aabb[4 * i + 3], __uint_as_float(g), 0.f, 0.f);
   }
@@ -118,11 +130,10 @@ struct SbWalk {  // a superblock list filtered to one tile (ballot compaction ke
   }
 };
 
-// q = d^T K d exactly as the reference's mult_vec_from_both_sides orders it:
-// (A dx) dx + B (dx dy + dy dx) + (C dy) dy
-__device__ __forceinline__ float quad(float B, float C, float dx, float dy, float adxdx) {
-  const float t = fm(dx, dy);
-  return fa(fa(adxdx, fm(B, fa(t, fm(dy, dx)))), fm(fm(C, dy), dy));
+// y = k q = (kA dx) dx + (k2B dx + kC dy) dy with the conic terms staged
+// pre-scaled: kadxdx = (kA dx) dx and kb2dx = k2B dx are per entry and lane.
+__device__ __forceinline__ float quad_y(float kC, float dy, float kb2dx, float kadxdx) {
+  return ff(ff(kC, dy, kb2dx), dy, kadxdx);
 }
 
 // ---------------------------------------------------------------------------
@@ -174,7 +185,8 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
         const float4 ea = sm[j].a, eb = sm[j].b, ec = sm[j].c, ed = sm[j].d;
         if (!(ec.y <= fx && fx <= ec.w)) continue;
         const float dx = fs(fx, ea.x);
-        const float adxdx = fm(fm(ea.z, dx), dx);
+        const float kadxdx = fm(fm(ea.z, dx), dx);
+        const float kb2dx = fm(ea.w, dx);
         const uint32_t pos = __float_as_uint(ed.z);
 #pragma unroll
         for (int k = 0; k < PPL; ++k) {
@@ -183,13 +195,12 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
           const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
           if (!(ec.z <= fy && fy <= ed.x)) continue;
           const float dy = fs(fy, ea.y);
-          const float q = quad(ea.w, eb.x, dx, dy, adxdx);
-          const float al = fm(dexp(fm(-0.5f, q)), eb.y);
+          const float al = fm(exp2_det(quad_y(eb.x, dy, kb2dx, kadxdx)), eb.y);
           const float eo = fm(T[k], al);
-          c0[k] = fa(c0[k], fm(eb.z, eo));
-          c1[k] = fa(c1[k], fm(eb.w, eo));
-          c2[k] = fa(c2[k], fm(ec.x, eo));
-          T[k] = fm(T[k], fs(1.f, al));
+          c0[k] = ff(eb.z, eo, c0[k]);
+          c1[k] = ff(eb.w, eo, c1[k]);
+          c2[k] = ff(ec.x, eo, c2[k]);
+          T[k] = fs(T[k], eo);
           as[k] = fa(as[k], eo);
           if (as[k] >= kAlphaBreak) {
             live &= ~(1u << k);
@@ -243,12 +254,12 @@ __device__ __forceinline__ ItemGeo item_geo(const ViewBatch& b, uint32_t item, c
   const ViewDev& vd = b.v[g.v];
   const uint32_t t = item - vd.item_base;
   const uint32_t tx = t % uint32_t(vd.tile_w), ty = t / uint32_t(vd.tile_w);
-  const uint32_t sbw = uint32_t(vd.tile_w + 7) >> 3;
-  const uint32_t sb = vd.sb_base + (ty >> 3) * sbw + (tx >> 3);
+  const int sl = vd.sb_log2;
+  const uint32_t sb = vd.sb_base + (ty >> sl) * uint32_t(sb_cols(vd)) + (tx >> sl);
   g.s = uint32_t(min(uint64_t(off1[size_t(sb) * nchunk]), capacity));
   g.e = uint32_t(min(uint64_t(off1[size_t(sb + 1) * nchunk]), capacity));
-  g.lx = tx & 7u;
-  g.ly = ty & 7u;
+  g.lx = tx & ((1u << sl) - 1u);
+  g.ly = ty & ((1u << sl) - 1u);
   g.px0 = int(tx) * b.ts;
   g.py0 = int(ty) * b.ts;
   return g;
@@ -342,14 +353,16 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     const int iy0 = ig.py0 + int(slab) * G::SLAB_ROWS + (lane / TS);
     const float fx = float(ix) + 0.5f;
     const uint32_t s = ig.s, e = ig.e;
-    float Tc[PPL], a0[PPL], a1[PPL], a2[PPL], d0[PPL], d1[PPL], d2[PPL];
+    // per pixel: T in front of the current entry, S = d . (colour behind it),
+    // d = dL/dpixel
+    float Tc[PPL], S[PPL], d0[PPL], d1[PPL], d2[PPL];
     uint32_t last[PPL];
     uint32_t lo_min = e;
 #pragma unroll
     for (int k = 0; k < PPL; ++k) {
       const int iy = iy0 + k * G::ROW_STEP;
-      a0[k] = a1[k] = a2[k] = 0.f;
       Tc[k] = 1.f;
+      S[k] = 0.f;
       d0[k] = d1[k] = d2[k] = 0.f;
       last[k] = e;  // outside pixels process nothing
       if (ix < vd.w && iy < vd.h) {
@@ -366,7 +379,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     for (int o = 16; o > 0; o >>= 1) lo_min = min(lo_min, __shfl_xor_sync(0xffffffffu, lo_min, o));
     PackedSrc src{rec + 3 * size_t(ig.v) * n};
     SbWalk walk{list1, ig.lx, ig.ly};
-    float4* gv = grad2d + 3 * size_t(ig.v) * n;
+    float* gv = reinterpret_cast<float*>(grad2d + 3 * size_t(ig.v) * n);
     for (uint32_t lo = max(s, lo_min); lo < e; lo += 32) {
       const int cnt = int(min(32u, e - lo));
       const int k_staged = walk.stage(src, sm, lo + uint32_t(lane), lane < cnt, lane);
@@ -374,60 +387,85 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
       for (int j = 0; j < k_staged; ++j) {
         const float4 ea = sm[j].a, eb = sm[j].b, ec = sm[j].c, ed = sm[j].d;
         const uint32_t pos = __float_as_uint(ed.z);
-        float gpx = 0.f, gpy = 0.f, gA = 0.f, gB = 0.f, gC = 0.f, gop = 0.f, gr = 0.f, gg = 0.f, gb = 0.f;
+        // v[]: this lane's sums over its pixels of (w dx, w dy, w dx^2,
+        // w dx dy, w dy^2, dL/dop, dL/dr, dL/dg) with w = dL/dq; gb = dL/db
+        float v[8], gb = 0.f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = 0.f;
         bool any = false;
+        const float dx = fx - ea.x;
         if (ec.y <= fx && fx <= ec.w) {
-          const float A = ea.z, B = ea.w, C = eb.x, op = eb.y;
-          const float dx = fs(fx, ea.x);
-          const float adxdx = fm(fm(A, dx), dx);
+          const float kadxdx = ea.z * dx * dx, kb2dx = ea.w * dx;
+          const float mhop = -0.5f * eb.y;
+          float sw = 0.f, swdy = 0.f, swdyy = 0.f;
 #pragma unroll
           for (int k = 0; k < PPL; ++k) {
             const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
             if (pos < last[k] || !(ec.z <= fy && fy <= ed.x)) continue;
             any = true;
-            const float dy = fs(fy, ea.y);
-            const float q = quad(B, C, dx, dy, adxdx);
-            const float Gv = __expf(-0.5f * q);
-            const float al = Gv * op;
-            const float iom = __frcp_rn(1.f - al);
-            Tc[k] = Tc[k] * iom;
+            const float dy = fy - ea.y;
+            const float Gv = ex2_approx(quad_y(eb.x, dy, kb2dx, kadxdx));
+            const float al = Gv * eb.y;
+            const float iom = rcp_approx(1.f - al);
+            Tc[k] *= iom;
             const float wgt = al * Tc[k];
-            const float dLde = d0[k] * (eb.z * Tc[k] - a0[k] * iom) + d1[k] * (eb.w * Tc[k] - a1[k] * iom) +
-                               d2[k] * (ec.x * Tc[k] - a2[k] * iom);
-            a0[k] += eb.z * wgt;
-            a1[k] += eb.w * wgt;
-            a2[k] += ec.x * wgt;
-            gr += wgt * d0[k];
-            gg += wgt * d1[k];
+            const float drgb = d0[k] * eb.z + d1[k] * eb.w + d2[k] * ec.x;
+            const float dLde = Tc[k] * drgb - iom * S[k];
+            S[k] += wgt * drgb;
+            v[6] += wgt * d0[k];
+            v[7] += wgt * d1[k];
             gb += wgt * d2[k];
-            gop += Gv * dLde;
-            const float dLdq = dLde * op * Gv * -0.5f;
-            gA += dLdq * dx * dx;
-            gB += dLdq * 2.f * dx * dy;
-            gC += dLdq * dy * dy;
-            gpx -= dLdq * (2.f * A * dx + 2.f * B * dy);
-            gpy -= dLdq * (2.f * B * dx + 2.f * C * dy);
+            const float t = Gv * dLde;
+            v[5] += t;
+            const float w = t * mhop;
+            const float wdy = w * dy;
+            sw += w;
+            swdy += wdy;
+            swdyy += wdy * dy;
           }
+          v[0] = sw * dx;
+          v[1] = swdy;
+          v[2] = v[0] * dx;
+          v[3] = swdy * dx;
+          v[4] = swdyy;
         }
         if (__any_sync(0xffffffffu, any)) {
+          // transposed butterfly: after the offset-16/8/4 steps lane L holds a
+          // partial sum of v[L >> 2]; offsets 2 and 1 finish it
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            gpx += __shfl_xor_sync(0xffffffffu, gpx, o);
-            gpy += __shfl_xor_sync(0xffffffffu, gpy, o);
-            gA += __shfl_xor_sync(0xffffffffu, gA, o);
-            gB += __shfl_xor_sync(0xffffffffu, gB, o);
-            gC += __shfl_xor_sync(0xffffffffu, gC, o);
-            gop += __shfl_xor_sync(0xffffffffu, gop, o);
-            gr += __shfl_xor_sync(0xffffffffu, gr, o);
-            gg += __shfl_xor_sync(0xffffffffu, gg, o);
-            gb += __shfl_xor_sync(0xffffffffu, gb, o);
+          for (int i = 0; i < 4; ++i) {
+            const bool up = lane & 16;
+            const float send = up ? v[i] : v[i + 4], keep = up ? v[i + 4] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
           }
-          if (lane == 0) {
-            float4* dst = gv + 3 * size_t(__float_as_uint(ed.y));
-            atomicAdd(dst, make_float4(gpx, gpy, gA, gB));
-            atomicAdd(dst + 1, make_float4(gC, gop, gr, gg));
-            atomicAdd(reinterpret_cast<float*>(dst + 2), gb);
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const bool up = lane & 8;
+            const float send = up ? v[i] : v[i + 2], keep = up ? v[i + 2] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
           }
+          {
+            const bool up = lane & 4;
+            const float send = up ? v[0] : v[1], keep = up ? v[1] : v[0];
+            v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+          }
+          v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
+          v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) gb += __shfl_xor_sync(0xffffffffu, gb, o);
+          const float m0 = __shfl_sync(0xffffffffu, v[0], 0), m1 = __shfl_sync(0xffffffffu, v[0], 4);
+          // d px = -2 (A m0 + B m1), d py = -2 (B m0 + C m1), d A = m2,
+          // d B = 2 m3, d C = m4 (raw conic recovered from the staged one)
+          const float A = ea.z * kInvNegHalfLog2e, B = ea.w * (0.5f * kInvNegHalfLog2e),
+                      C = eb.x * kInvNegHalfLog2e;
+          const int k = lane >> 2;
+          float out = v[0];
+          if (k == 0) out = -2.f * (A * m0 + B * m1);
+          if (k == 1) out = -2.f * (B * m0 + C * m1);
+          if (k == 3) out = 2.f * v[0];
+          float* dst = gv + 12 * size_t(__float_as_uint(ed.y));
+          if ((lane & 3) == 0) atomicAdd(dst + k, out);
+          if (lane == 1) atomicAdd(dst + 8, gb);
         }
       }
       __syncwarp();

@@ -7,16 +7,20 @@
 // scan and sort taken from the absent del-cudarc-sys crate.
 //
 // Design here (same result, fewer bytes moved):
-//   1. depth sort: the N per-point depth keys are sorted once (stable, so
-//      equal depths stay in point-index order) -> a rank per point;
-//   2. pairs are emitted in rank order (exclusive scan of the per-point
-//      counts taken in rank order gives each point's output run);
-//   3. a stable LSD sort of the pairs by tile id alone (8-bit digits over
-//      ceil(log2(#tiles)) bits) -- stability keeps rank order inside a tile.
-// The result is the reference's order, (tile, depth bits, point index)
-// ascending, i.e. the same tile2idx / idx2pnt bit for bit, while the P-sized
-// sort touches 8 bytes per pair per pass over ~2 passes instead of 12 bytes
-// over 5-7 passes.
+//   1. depth sort: each view's N depth keys are sorted once by a stable
+//      segmented LSD radix sort (equal depths stay in point-index order) ->
+//      the points of every view in rank order;
+//   2. stage 1: a stable multisplit of that rank sequence into superblock
+//      lists (square blocks of 1, 2, 4 or 8 tiles per side, chosen per view):
+//      per (chunk, superblock) counts, one exclusive scan, then a scatter
+//      whose in-warp slots come from ballots; an entry is (point, its tile
+//      span clipped to the superblock).  The batched rasteriser walks these
+//      lists directly, filtering by tile;
+//   3. stage 2 (reference-format output only): one CTA per superblock splits
+//      its list into per-tile lists with ballot ranking -> tile2idx/idx2pnt.
+// Filtering a rank-ordered superblock list by tile keeps rank order, so every
+// tile list is the reference's order, (tile, depth bits, point index)
+// ascending, bit for bit; no 64-bit pair key is sorted.
 #include "common.cuh"
 
 namespace dsplat {
@@ -267,23 +271,24 @@ __global__ void k_iota_pad(uint32_t* __restrict__ vals, uint32_t* __restrict__ k
   if (r >= n) keys[i] = 0xffffffffu;
 }
 
-// superblock span of a tile span (8x8 tiles per superblock); empty if no tile
-__device__ __forceinline__ bool sb_span(uint2 rc, int* sx0, int* sy0, int* sx1, int* sy1) {
+// superblock span of a tile span (superblocks of 1 << sl tiles per side);
+// empty if no tile
+__device__ __forceinline__ bool sb_span(uint2 rc, int sl, int* sx0, int* sy0, int* sx1, int* sy1) {
   const int x0 = rc.x & 0xffff, y0 = rc.x >> 16, x1 = rc.y & 0xffff, y1 = rc.y >> 16;
   if (x1 <= x0 || y1 <= y0) return false;
-  *sx0 = x0 >> 3;
-  *sy0 = y0 >> 3;
-  *sx1 = ((x1 - 1) >> 3) + 1;
-  *sy1 = ((y1 - 1) >> 3) + 1;
+  *sx0 = x0 >> sl;
+  *sy0 = y0 >> sl;
+  *sx1 = ((x1 - 1) >> sl) + 1;
+  *sy1 = ((y1 - 1) >> sl) + 1;
   return true;
 }
 
-// tile span clipped to superblock (sx, sy), in local tile coordinates 0..8:
-// x0 | y0 << 4 | x1 << 8 | y1 << 12
-__device__ __forceinline__ uint32_t local_rect(uint2 rc, int sx, int sy) {
-  const int bx = sx * 8, by = sy * 8;
-  const int x0 = max(int(rc.x & 0xffff), bx) - bx, x1 = min(int(rc.y & 0xffff), bx + 8) - bx;
-  const int y0 = max(int(rc.x >> 16), by) - by, y1 = min(int(rc.y >> 16), by + 8) - by;
+// tile span clipped to superblock (sx, sy), in local tile coordinates
+// 0..(1 << sl): x0 | y0 << 4 | x1 << 8 | y1 << 12
+__device__ __forceinline__ uint32_t local_rect(uint2 rc, int sl, int sx, int sy) {
+  const int side = 1 << sl, bx = sx << sl, by = sy << sl;
+  const int x0 = max(int(rc.x & 0xffff), bx) - bx, x1 = min(int(rc.y & 0xffff), bx + side) - bx;
+  const int y0 = max(int(rc.x >> 16), by) - by, y1 = min(int(rc.y >> 16), by + side) - by;
   return uint32_t(x0) | uint32_t(y0) << 4 | uint32_t(x1) << 8 | uint32_t(y1) << 12;
 }
 
@@ -306,7 +311,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restr
   const uint32_t nchunk = npad / kMsChunk;
   const uint32_t v = blockIdx.x / nchunk, c = blockIdx.x % nchunk;
   const ViewDev& vd = b.v[v];
-  const int sbw = (vd.tile_w + 7) >> 3, sbh = (vd.tile_h + 7) >> 3;
+  const int sl = vd.sb_log2, sbw = sb_cols(vd), sbh = sb_rows(vd);
   const int nsb = sbw * sbh;
   for (int i = threadIdx.x; i < nsb; i += kMsThreads) hist[i] = 0;
   __syncthreads();
@@ -317,7 +322,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restr
     if (g >= n) continue;
     const uint2 rc = rect[size_t(v) * n + g];
     int sx0, sy0, sx1, sy1;
-    if (!sb_span(rc, &sx0, &sy0, &sx1, &sy1)) continue;
+    if (!sb_span(rc, sl, &sx0, &sy0, &sx1, &sy1)) continue;
     pairs += uint32_t((rc.y & 0xffff) - (rc.x & 0xffff)) * uint32_t((rc.y >> 16) - (rc.x >> 16));
     for (int sy = sy0; sy < sy1; ++sy)
       for (int sx = sx0; sx < sx1; ++sx) atomicAdd(&hist[sy * sbw + sx], 1u);
@@ -347,7 +352,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
   const uint32_t nchunk = npad / kMsChunk;
   const uint32_t v = blockIdx.x / nchunk, c = blockIdx.x % nchunk;
   const ViewDev& vd = b.v[v];
-  const int sbw = (vd.tile_w + 7) >> 3, sbh = (vd.tile_h + 7) >> 3;
+  const int sl = vd.sb_log2, sbw = sb_cols(vd), sbh = sb_rows(vd);
   const int nsb = sbw * sbh;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
@@ -362,7 +367,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
   for (int r = 0; r < kMsRounds; ++r) {
     const uint32_t g = order[base + r * 32 + lane];
     int sx0, sy0, sx1, sy1;
-    if (g < n && sb_span(rect[size_t(v) * n + g], &sx0, &sy0, &sx1, &sy1))
+    if (g < n && sb_span(rect[size_t(v) * n + g], sl, &sx0, &sy0, &sx1, &sy1))
       for (int sy = sy0; sy < sy1; ++sy)
         for (int sx = sx0; sx < sx1; ++sx) atomicAdd(&my[sy * sbw + sx], 1u);
   }
@@ -383,7 +388,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
     const uint32_t g = order[base + r * 32 + lane];
     int sx0 = 0, sy0 = 0, sx1 = 0, sy1 = 0;
     const uint2 rc = g < n ? rect[size_t(v) * n + g] : make_uint2(0u, 0u);
-    const bool has = g < n && sb_span(rc, &sx0, &sy0, &sx1, &sy1);
+    const bool has = g < n && sb_span(rc, sl, &sx0, &sy0, &sx1, &sy1);
     // the round's column / row coverage masks
     int cx0 = has ? sx0 : 255, cx1 = has ? sx1 : 0, cy0 = has ? sy0 : 255, cy1 = has ? sy1 : 0;
 #pragma unroll
@@ -407,7 +412,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
       for (int sx = sx0; sx < sx1; ++sx) {
         const uint32_t m = colmask[sx] & rm;
         const uint32_t dst = my[sy * sbw + sx] + uint32_t(__popc(m & lt));
-        if (dst < capacity) list1[dst] = make_uint2(g, local_rect(rc, sx, sy));
+        if (dst < capacity) list1[dst] = make_uint2(g, local_rect(rc, sl, sx, sy));
         else set_flag(flags, kFlagPairOverflow);
       }
     }
@@ -442,9 +447,9 @@ __global__ void __launch_bounds__(kMsThreads) k_tile_count(const uint2* __restri
   const uint32_t sb = blockIdx.x;
   const int v = view_of_sb(b, sb);
   const ViewDev& vd = b.v[v];
-  const int sbw = (vd.tile_w + 7) >> 3;
+  const int sl = vd.sb_log2, side = 1 << sl, sbw = sb_cols(vd);
   const uint32_t ls = sb - vd.sb_base;
-  const int tx0 = int(ls % uint32_t(sbw)) * 8, ty0 = int(ls / uint32_t(sbw)) * 8;
+  const int tx0 = int(ls % uint32_t(sbw)) << sl, ty0 = int(ls / uint32_t(sbw)) << sl;
   if (threadIdx.x < 64) h[threadIdx.x] = 0;
   __syncthreads();
   const uint64_t s = min(uint64_t(off1[size_t(sb) * nchunk]), capacity);
@@ -456,7 +461,7 @@ __global__ void __launch_bounds__(kMsThreads) k_tile_count(const uint2* __restri
       for (int x = x0; x < x1; ++x) atomicAdd(&h[y * 8 + x], 1u);
   }
   __syncthreads();
-  if (threadIdx.x < 64) {
+  if (threadIdx.x < 64 && int(threadIdx.x & 7) < side && int(threadIdx.x >> 3) < side) {
     const int x = tx0 + (threadIdx.x & 7), y = ty0 + (threadIdx.x >> 3);
     if (x < vd.tile_w && y < vd.tile_h) tcnt[vd.item_base + uint32_t(y) * vd.tile_w + x] = h[threadIdx.x];
   }
@@ -483,14 +488,15 @@ __global__ void __launch_bounds__(kMsThreads) k_tile_scatter(const uint2* __rest
   const uint32_t sb = blockIdx.x;
   const int v = view_of_sb(b, sb);
   const ViewDev& vd = b.v[v];
-  const int sbw = (vd.tile_w + 7) >> 3;
+  const int sl = vd.sb_log2, side = 1 << sl, sbw = sb_cols(vd);
   const uint32_t ls = sb - vd.sb_base;
-  const int tx0 = int(ls % uint32_t(sbw)) * 8, ty0 = int(ls / uint32_t(sbw)) * 8;
+  const int tx0 = int(ls % uint32_t(sbw)) << sl, ty0 = int(ls / uint32_t(sbw)) << sl;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
   if (threadIdx.x < 64) {
     const int x = tx0 + (threadIdx.x & 7), y = ty0 + (threadIdx.x >> 3);
-    run[threadIdx.x] = (x < vd.tile_w && y < vd.tile_h) ? item_start[vd.item_base + uint32_t(y) * vd.tile_w + x] : 0u;
+    const bool in = int(threadIdx.x & 7) < side && int(threadIdx.x >> 3) < side && x < vd.tile_w && y < vd.tile_h;
+    run[threadIdx.x] = in ? item_start[vd.item_base + uint32_t(y) * vd.tile_w + x] : 0u;
   }
   __syncthreads();
   const uint64_t s = min(uint64_t(off1[size_t(sb) * nchunk]), capacity);
@@ -510,6 +516,7 @@ __global__ void __launch_bounds__(kMsThreads) k_tile_scatter(const uint2* __rest
 #pragma unroll
     for (int k = 0; k < 64; ++k) {
       const int kx = k & 7, ky = k >> 3;
+      if (kx >= side || ky >= side) continue;  // outside a smaller superblock
       const uint32_t m = __ballot_sync(0xffffffffu, kx >= x0 && kx < x1 && ky >= y0 && ky < y1);
       if ((k & 31) == lane) masks[warp][k] = m;
     }
@@ -559,7 +566,7 @@ __device__ __forceinline__ uint32_t item_cost_bucket(const ViewBatch& b, uint32_
   const ViewDev& vd = b.v[v];
   const uint32_t t = item - vd.item_base;
   const uint32_t tx = t % uint32_t(vd.tile_w), ty = t / uint32_t(vd.tile_w);
-  const uint32_t sb = vd.sb_base + (ty >> 3) * (uint32_t(vd.tile_w + 7) >> 3) + (tx >> 3);
+  const uint32_t sb = vd.sb_base + (ty >> vd.sb_log2) * uint32_t(sb_cols(vd)) + (tx >> vd.sb_log2);
   const uint32_t len = off1[size_t(sb + 1) * nchunk] - off1[size_t(sb) * nchunk];
   return len ? uint32_t(__clz(len)) : 32u;  // 0 = longest
 }

@@ -54,7 +54,7 @@ class BatchLayout(ctypes.Structure):
                 ("off_flags", c_size), ("off_rec", c_size), ("off_rect", c_size), ("off_cnt", c_size),
                 ("off_order", c_size), ("off_sb_start", c_size), ("off_sb_list", c_size),
                 ("off_pix_T", c_size), ("off_pix_stop", c_size), ("off_grad_pix", c_size),
-                ("off_slab_loss", c_size), ("off_grad2d", c_size)]
+                ("off_slab_loss", c_size), ("off_grad2d", c_size), ("sb_log2", c_i32 * 32)]
 
 
 _P = c_void_p  # every pointer is passed as an integer address

@@ -157,13 +157,15 @@ class GaussBatch:
         stop [H,W] i64 = each pixel's stop position as an idx2pnt position)."""
         L = self.layout
         ts = self.tile_size
-        sb_base = 0
-        for c in self.cameras[:view]:
-            tw_, th_ = (c.width + ts - 1) // ts, (c.height + ts - 1) // ts
-            sb_base += ((tw_ + 7) // 8) * ((th_ + 7) // 8)
+
+        def grid(v):
+            tw_, th_ = (self.cameras[v].width + ts - 1) // ts, (self.cameras[v].height + ts - 1) // ts
+            side_ = 1 << int(L.sb_log2[v])
+            return tw_, th_, side_, (tw_ + side_ - 1) // side_, (th_ + side_ - 1) // side_
+
+        sb_base = sum(grid(v)[3] * grid(v)[4] for v in range(view))
         c = self.cameras[view]
-        tw, th = (c.width + ts - 1) // ts, (c.height + ts - 1) // ts
-        sbw = (tw + 7) // 8
+        tw, th, side, sbw, _ = grid(view)
         ch = int(L.sb_chunks)
         starts = self._ws(L.off_sb_start, int(L.num_sb) * ch + 1, torch.int32).cpu().numpy().view(np.uint32)
         ent = self._ws(L.off_sb_list, 2 * self.capacity, torch.int32).cpu().numpy().view(np.uint32).reshape(-1, 2)
@@ -172,10 +174,10 @@ class GaussBatch:
         lists, positions = [], []
         for t in range(tw * th):
             tx, ty = t % tw, t // tw
-            sb = sb_base + (ty // 8) * sbw + (tx // 8)
+            sb = sb_base + (ty // side) * sbw + (tx // side)
             s, e = int(starts[sb * ch]), int(starts[(sb + 1) * ch])
             lr = ent[s:e, 1]
-            lx, ly = tx % 8, ty % 8
+            lx, ly = tx % side, ty % side
             m = (lx >= (lr & 15)) & (lx < ((lr >> 8) & 15)) & (ly >= ((lr >> 4) & 15)) & (ly < (lr >> 12))
             lists.append(ent[s:e, 0][m])
             positions.append(s + np.nonzero(m)[0])

@@ -172,7 +172,8 @@ typedef struct { /* gradients, accumulated (+=) */
 
 /* Byte offsets of the batch state inside the workspace (for inspection).
  * Tile lists of the batched path live in superblock form: superblock s
- * (8x8 tiles; view v's superblocks start at the sum of the earlier views'
+ * (square blocks of 2^sb_log2[v] tiles per side, chosen per view from its
+ * tile grid; view v's superblocks start at the sum of the earlier views'
  * counts, row-major inside the view) owns the entries
  * sb_list[sb_start[s * sb_chunks] .. sb_start[(s + 1) * sb_chunks]), each a
  * (point index, span) pair where span packs the tiles it covers inside the
@@ -198,6 +199,7 @@ typedef struct {
   size_t off_grad_pix;   /* f32[num_pix*3] dL/dpixel (loss gradient) */
   size_t off_slab_loss;  /* f32[num_items*slabs_per_tile] partial L2 losses */
   size_t off_grad2d;     /* float4[V*N*3] per-view 2D gradients */
+  int32_t sb_log2[32];   /* per view: superblock side = 1 << sb_log2 tiles (0..3) */
 } dsplat_batch_layout;
 
 /* tile_size: 8, 16 or 32.  pixels_per_lane: rasteriser work split, one warp

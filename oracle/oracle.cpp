@@ -242,6 +242,54 @@ inline float dexp_f32(float x) {
   return p * sc;
 }
 
+// Deterministic 2^y, identical operation for operation to the CUDA
+// exp2_det(): y = n + f with n the nearest integer (adding 1.5 * 2^23 rounds
+// y where the float spacing is 1; n is read from the sum's bits), |f| <= 1/2,
+// the degree-6 Taylor polynomial of e^(f ln 2) in Horner form with fused
+// multiply-adds (std::fma is exactly rounded, like the GPU's fma), and exact
+// scaling by 2^n through the exponent field.  Outside (-125, 123): 0 below,
+// +inf above, NaN stays NaN.
+inline float exp2_det_f32(float y) {
+  if (!(std::fabs(y + 1.f) < 124.f)) {
+    if (y != y) return y;
+    return y < 0.f ? 0.f : INFINITY;
+  }
+  const float t = y + 12582912.f;
+  const float f = y - (t - 12582912.f);
+  float p = 1.5403530393381608e-4f;
+  p = std::fma(p, f, 1.3333558146428443e-3f);
+  p = std::fma(p, f, 9.6181291076284772e-3f);
+  p = std::fma(p, f, 5.5504108664821580e-2f);
+  p = std::fma(p, f, 2.4022650695910071e-1f);
+  p = std::fma(p, f, 6.9314718055994531e-1f);
+  p = std::fma(p, f, 1.f);
+  uint32_t tb, pb, magic;
+  const float m = 12582912.f;
+  std::memcpy(&tb, &t, 4);
+  std::memcpy(&pb, &p, 4);
+  std::memcpy(&magic, &m, 4);
+  const uint32_t r = pb + ((tb - magic) << 23);
+  float out;
+  std::memcpy(&out, &r, 4);
+  return out;
+}
+
+// exp(-q/2) * opacity for the blend, as the CUDA rasterisers evaluate it:
+// the conic is pre-scaled by k = -log2(e)/2 (kA, k2B, kC), then
+// y = (kA dx) dx + (k2B dx + kC dy) dy with two fused multiply-adds and
+// alpha = 2^y * opacity.  splat_gauss.cu:96-98 computes the same quantity as
+// exp(-0.5 * (A dx dx + B (dx dy + dy dx) + C dy dy)) * opacity; the two
+// differ only in rounding.
+constexpr float kNegHalfLog2e = -0.72134752044448170368f;
+inline float blend_alpha(const float* conic, float opacity, float dx, float dy) {
+  const float ka = conic[0] * kNegHalfLog2e;
+  const float kb2 = (conic[1] + conic[1]) * kNegHalfLog2e;
+  const float kc = conic[2] * kNegHalfLog2e;
+  const float kadxdx = (ka * dx) * dx, kb2dx = kb2 * dx;
+  const float y = std::fma(std::fma(kc, dy, kb2dx), dy, kadxdx);
+  return exp2_det_f32(y) * opacity;
+}
+
 // splat_gauss.cu:105: `alpha_sum > 0.999` compares in double; for a float
 // alpha_sum that is exactly `alpha_sum >= 0.999f` (0.999f > 0.999).
 constexpr float kAlphaBreak = 0.999f;
@@ -493,14 +541,12 @@ inline int32_t blend_pixel(int ix, int iy, uint32_t start, uint32_t end,
     const uint32_t g = idx2pnt[pos];
     if (!in_aabb(aabb + 4 * g, tx, ty)) continue;
     const float dx = tx - xyd[3 * g], dy = ty - xyd[3 * g + 1];
-    const float* k = conic + 3 * g;
-    const float q = k[0] * dx * dx + k[1] * (dx * dy + dy * dx) + k[2] * dy * dy;
-    const float e = dexp_f32(-0.5f * q) * opacity[g];
+    const float e = blend_alpha(conic + 3 * g, opacity[g], dx, dy);
     const float eo = occ * e;
-    c0 += rgb[3 * g + 0] * eo;
-    c1 += rgb[3 * g + 1] * eo;
-    c2 += rgb[3 * g + 2] * eo;
-    occ *= 1.f - e;
+    c0 = std::fma(rgb[3 * g + 0], eo, c0);
+    c1 = std::fma(rgb[3 * g + 1], eo, c1);
+    c2 = std::fma(rgb[3 * g + 2], eo, c2);
+    occ = occ - eo;
     asum += eo;
     if (asum >= kAlphaBreak) {
       last = int32_t(pos);
@@ -557,14 +603,12 @@ extern "C" void orc_gauss_render_naive(int64_t n, const float* xyd,
         if (z <= -1.f || z >= 1.f) continue;
         if (!in_aabb(aabb + 4 * g, tx, ty)) continue;
         const float dx = tx - xyd[3 * g], dy = ty - xyd[3 * g + 1];
-        const float* k = conic + 3 * g;
-        const float q = k[0] * dx * dx + k[1] * (dx * dy + dy * dx) + k[2] * dy * dy;
-        const float e = dexp_f32(-0.5f * q) * opacity[g];
+        const float e = blend_alpha(conic + 3 * g, opacity[g], dx, dy);
         const float eo = occ * e;
-        o[0] += rgb[3 * g + 0] * eo;
-        o[1] += rgb[3 * g + 1] * eo;
-        o[2] += rgb[3 * g + 2] * eo;
-        occ *= 1.f - e;
+        o[0] = std::fma(rgb[3 * g + 0], eo, o[0]);
+        o[1] = std::fma(rgb[3 * g + 1], eo, o[1]);
+        o[2] = std::fma(rgb[3 * g + 2], eo, o[2]);
+        occ = occ - eo;
         asum += eo;
         if (asum >= kAlphaBreak) break;
       }
