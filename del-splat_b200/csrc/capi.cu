@@ -18,8 +18,10 @@ __global__ void k_prep_tiles(uint32_t, const float*, const float*, const float*,
                              uint32_t*);
 __global__ void k_fused_project(uint32_t, uint32_t, int, const float*, const float*, const float*, const float*,
                                 const float*, const ViewBatch, float4*, uint2*, uint32_t*, uint32_t*);
-__global__ void k_project_bwd(uint32_t, int, const float*, const float*, const float*, const float*, const ViewBatch,
-                              const float4*, float*, float*, float*, float*, float*);
+__global__ void k_project_bwd_geom(uint32_t, const float*, const float*, const float*, const ViewBatch,
+                                   const float4*, float*, float*, float*, float*);
+__global__ void k_project_bwd_colour(uint32_t, int, const float*, const float*, const ViewBatch, const float4*,
+                                     float*, float*);
 __global__ void k_adam(size_t, float*, const float*, float*, float*, float, float, float, float, float, float);
 __global__ void k_iota_pad(uint32_t*, uint32_t*, uint32_t, uint32_t, uint32_t);
 __global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*, uint32_t*);
@@ -711,9 +713,13 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
   TRY_CUDA(raster_bwd(st, b, ba),
            "raster_bwd");
   stage_mark(st, 8);
-  k_project_bwd<<<blocks_for(n, 128), 128, 0, st>>>(n, params->sh_degree, params->means, params->log_scales,
-                                                    params->quats, params->colors, b, w.grad2d, grads->means,
-                                                    grads->log_scales, grads->quats, grads->opacity, grads->colors); count_launch();
+  k_project_bwd_geom<<<blocks_for(n, 128), 128, 0, st>>>(n, params->means, params->log_scales, params->quats, b,
+                                                         w.grad2d, grads->means, grads->log_scales, grads->quats,
+                                                         grads->opacity);
+  count_launch();
+  k_project_bwd_colour<<<blocks_for(n, 128), 128, 0, st>>>(n, params->sh_degree, params->means, params->colors, b,
+                                                           w.grad2d, grads->means, grads->colors);
+  count_launch();
   stage_mark(st, 9);
   TRY_CUDA(cudaGetLastError(), "backward");
   return DSPLAT_OK;
