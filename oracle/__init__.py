@@ -232,6 +232,8 @@ class Scene:
 
     def __init__(self, means, log_scales, quats, opacity, colors, sh_deg, mvp, campos, w, h, ts,
                  tile2idx, idx2pnt, pix_last, aabb, target):
+        if int(ts) <= 0 or int(w) <= 0 or int(h) <= 0:
+            raise ValueError(f"oracle Scene: tile size and image size must be positive (ts={ts}, {w}x{h})")
         self.a = dict(
             means=f32(means), log_scales=f32(log_scales), quats=f32(quats), opacity=f32(opacity).reshape(-1),
             colors=f32(colors), mvp=f32(mvp).reshape(16), campos=f32(campos).reshape(3),
