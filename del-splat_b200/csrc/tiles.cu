@@ -125,118 +125,132 @@ cudaError_t exclusive_scan(cudaStream_t st, const uint32_t* in, uint32_t* out, s
 
 // ---------------------------------------------------------------------------
 // Stable LSD radix sort of (u32 key, u32 value), 8-bit digits.
-// Each block owns a tile of 4096 consecutive elements (8 warps x 16 rounds x
-// 32 lanes, in index order).  Segmented form: with nb_seg blocks per segment
-// the histogram is laid out (segment, digit, block) so that one exclusive scan
-// yields every element's destination and segments never mix.
+// Each block owns a tile of 4096 consecutive elements.  Segmented form: with
+// nb_seg blocks per segment the histogram is laid out (segment, digit, block)
+// so that one exclusive scan yields every block's output offset per digit and
+// segments never mix.
+//   upsweep:   16-byte key loads, per-warp shared histograms;
+//   downsweep: warp w ranks its 512 elements (16 rounds of 32, in index
+//              order) with match_any; the block turns the per-warp counts
+//              into local digit offsets, scatters (key, value) into shared
+//              memory in digit order, and writes each digit's run to its
+//              global offset with consecutive threads on consecutive
+//              addresses.
 // ---------------------------------------------------------------------------
 constexpr int kRsThreads = 256;
 constexpr int kRsWarps = kRsThreads / 32;
 constexpr int kRsRounds = 16;
 constexpr int kRsTile = kRsThreads * kRsRounds;  // 4096
 
-__device__ __forceinline__ uint32_t live_count(size_t n, const uint32_t* count_ptr) {
-  if (!count_ptr) return uint32_t(n);
-  const uint32_t c = *count_ptr;
-  return c < n ? c : uint32_t(n);
-}
-
-__global__ void __launch_bounds__(kRsThreads) k_radix_upsweep(const uint32_t* __restrict__ keys, size_t n,
-                                                              const uint32_t* __restrict__ count_ptr, int shift,
+__global__ void __launch_bounds__(kRsThreads) k_radix_upsweep(const uint32_t* __restrict__ keys, int shift,
                                                               uint32_t nb_seg, uint32_t* __restrict__ hist) {
-  __shared__ uint32_t h[256];
-  h[threadIdx.x] = 0;
+  __shared__ uint32_t h[kRsWarps][256];
+  for (int i = threadIdx.x; i < kRsWarps * 256; i += kRsThreads) (&h[0][0])[i] = 0;
   __syncthreads();
-  const uint32_t cnt = live_count(n, count_ptr);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const size_t base = size_t(blockIdx.x) * kRsTile + size_t(warp) * (kRsRounds * 32);
-#pragma unroll 4
-  for (int r = 0; r < kRsRounds; ++r) {
-    const size_t idx = base + r * 32 + lane;
-    const bool valid = idx < cnt;
-    const uint32_t d = valid ? (keys[idx] >> shift) & 255u : 256u;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[d], __popc(peers));
+  const int warp = threadIdx.x >> 5;
+  const uint4* k4 = reinterpret_cast<const uint4*>(keys + size_t(blockIdx.x) * kRsTile);
+#pragma unroll
+  for (int r = 0; r < kRsTile / 4 / kRsThreads; ++r) {
+    const uint4 q = k4[r * kRsThreads + threadIdx.x];
+    atomicAdd(&h[warp][(q.x >> shift) & 255u], 1u);
+    atomicAdd(&h[warp][(q.y >> shift) & 255u], 1u);
+    atomicAdd(&h[warp][(q.z >> shift) & 255u], 1u);
+    atomicAdd(&h[warp][(q.w >> shift) & 255u], 1u);
   }
   __syncthreads();
+  uint32_t sum = 0;
+#pragma unroll
+  for (int w = 0; w < kRsWarps; ++w) sum += h[w][threadIdx.x];
   const uint32_t seg = blockIdx.x / nb_seg, b = blockIdx.x % nb_seg;
-  hist[(size_t(seg) * 256 + threadIdx.x) * nb_seg + b] = h[threadIdx.x];
+  hist[(size_t(seg) * 256 + threadIdx.x) * nb_seg + b] = sum;
 }
 
 __global__ void __launch_bounds__(kRsThreads) k_radix_downsweep(
     const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
-    uint32_t* __restrict__ vout, size_t n, const uint32_t* __restrict__ count_ptr, int shift, uint32_t nb_seg,
-    const uint32_t* __restrict__ offs) {
+    uint32_t* __restrict__ vout, int shift, uint32_t nb_seg, const uint32_t* __restrict__ offs, int write_keys) {
   __shared__ uint32_t wc[kRsWarps][256];
+  __shared__ uint32_t dstart[256];
+  __shared__ uint32_t goff[256];
+  __shared__ uint32_t sk[kRsTile];
+  __shared__ uint32_t sv[kRsTile];
 #pragma unroll
   for (int w = 0; w < kRsWarps; ++w) wc[w][threadIdx.x] = 0;
   __syncthreads();
-  const uint32_t cnt = live_count(n, count_ptr);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
   const size_t base = size_t(blockIdx.x) * kRsTile + size_t(warp) * (kRsRounds * 32);
   uint32_t k[kRsRounds], v[kRsRounds];
 #pragma unroll
   for (int r = 0; r < kRsRounds; ++r) {
-    const size_t idx = base + r * 32 + lane;
-    if (idx < cnt) {
-      k[r] = kin[idx];
-      v[r] = vin[idx];
-    } else {
-      k[r] = 0;
-      v[r] = 0;
-    }
+    k[r] = kin[base + r * 32 + lane];
+    v[r] = vin[base + r * 32 + lane];
   }
   // phase 1: per-warp digit counts
 #pragma unroll
   for (int r = 0; r < kRsRounds; ++r) {
-    const bool valid = base + r * 32 + lane < cnt;
-    const uint32_t d = valid ? (k[r] >> shift) & 255u : 256u;
+    const uint32_t d = (k[r] >> shift) & 255u;
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    if (valid && lane == __ffs(peers) - 1) wc[warp][d] += __popc(peers);
+    if (lane == __ffs(peers) - 1) wc[warp][d] += __popc(peers);
     __syncwarp();
   }
   __syncthreads();
-  // phase 2: warp bases = block offset of the digit + earlier warps
+  // phase 2: block-local digit starts, warp bases, global digit offsets
   {
     const uint32_t d = threadIdx.x;
-    const uint32_t seg = blockIdx.x / nb_seg, b = blockIdx.x % nb_seg;
-    uint32_t run = offs[(size_t(seg) * 256 + d) * nb_seg + b];
+    uint32_t tot = 0;
+#pragma unroll
+    for (int w = 0; w < kRsWarps; ++w) tot += wc[w][d];
+    uint32_t all;
+    uint32_t run = block_excl_scan(tot, &all);
+    dstart[d] = run;
 #pragma unroll
     for (int w = 0; w < kRsWarps; ++w) {
       const uint32_t t = wc[w][d];
       wc[w][d] = run;
       run += t;
     }
+    const uint32_t seg = blockIdx.x / nb_seg, b = blockIdx.x % nb_seg;
+    goff[d] = offs[(size_t(seg) * 256 + d) * nb_seg + b];
   }
   __syncthreads();
-  // phase 3: stable scatter
+  // phase 3: stable scatter into shared memory, digit-major
 #pragma unroll
   for (int r = 0; r < kRsRounds; ++r) {
-    const bool valid = base + r * 32 + lane < cnt;
-    const uint32_t d = valid ? (k[r] >> shift) & 255u : 256u;
+    const uint32_t d = (k[r] >> shift) & 255u;
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    const uint32_t rb = valid ? wc[warp][d] : 0u;
+    const uint32_t rb = wc[warp][d];
     __syncwarp();
-    if (valid && lane == __ffs(peers) - 1) wc[warp][d] = rb + __popc(peers);
+    if (lane == __ffs(peers) - 1) wc[warp][d] = rb + __popc(peers);
     __syncwarp();
-    if (valid) {
-      const uint32_t pos = rb + __popc(peers & lt);
-      kout[pos] = k[r];
-      vout[pos] = v[r];
-    }
+    const uint32_t lp = rb + __popc(peers & lt);
+    sk[lp] = k[r];
+    sv[lp] = v[r];
+  }
+  __syncthreads();
+  // phase 4: digit runs to their global offsets
+#pragma unroll 4
+  for (int i = threadIdx.x; i < kRsTile; i += kRsThreads) {
+    const uint32_t key = sk[i];
+    const uint32_t d = (key >> shift) & 255u;
+    const uint32_t pos = goff[d] + (uint32_t(i) - dstart[d]);
+    if (write_keys) kout[pos] = key;
+    vout[pos] = sv[i];
   }
 }
 
 size_t radix_hist_words(size_t n) { return ((n + kRsTile - 1) / kRsTile) * 256; }
 
 // Sorts (ka, va) by bits [0, nbits) of the key, ping-ponging with (kb, vb).
-// Returns in *result_in_b whether the sorted data ended in the b buffers.
-// n must be a multiple of 4096 per segment when nseg > 1.
+// Returns in *result_in_b whether the sorted values ended in the b buffers;
+// the keys of the last pass are not written (callers use the values only).
+// n must be a multiple of 4096 (per segment when nseg > 1); count_ptr must be
+// null (every element takes part).
 cudaError_t radix_sort(cudaStream_t st, uint32_t* ka, uint32_t* va, uint32_t* kb, uint32_t* vb, size_t n,
                        const uint32_t* count_ptr, int nbits, uint32_t nseg, uint32_t* hist, uint32_t* scan_tmp,
                        bool* result_in_b) {
-  const uint32_t nblocks = uint32_t((n + kRsTile - 1) / kRsTile);
+  if (n % kRsTile != 0 || count_ptr != nullptr || nseg == 0 || (n / kRsTile) % nseg != 0)
+    return cudaErrorInvalidValue;
+  const uint32_t nblocks = uint32_t(n / kRsTile);
   const uint32_t nb_seg = nblocks / nseg;
   const size_t hw = size_t(nblocks) * 256;
   bool in_b = false;
@@ -249,10 +263,12 @@ cudaError_t radix_sort(cudaStream_t st, uint32_t* ka, uint32_t* va, uint32_t* kb
     const uint32_t* vi = in_b ? vb : va;
     uint32_t* ko = in_b ? ka : kb;
     uint32_t* vo = in_b ? va : vb;
-    k_radix_upsweep<<<nblocks, kRsThreads, 0, st>>>(ki, n, count_ptr, shift, nb_seg, hist); count_launch();
+    k_radix_upsweep<<<nblocks, kRsThreads, 0, st>>>(ki, shift, nb_seg, hist); count_launch();
     cudaError_t e = exclusive_scan(st, hist, hist, hw, scan_tmp);
     if (e != cudaSuccess) return e;
-    k_radix_downsweep<<<nblocks, kRsThreads, 0, st>>>(ki, vi, ko, vo, n, count_ptr, shift, nb_seg, hist); count_launch();
+    const int last = shift + 8 >= nbits;
+    k_radix_downsweep<<<nblocks, kRsThreads, 0, st>>>(ki, vi, ko, vo, shift, nb_seg, hist, last ? 0 : 1);
+    count_launch();
     in_b = !in_b;
   }
   *result_in_b = in_b;
