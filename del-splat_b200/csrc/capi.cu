@@ -43,7 +43,7 @@ size_t scan_tmp_words(size_t n);
 size_t radix_hist_words(size_t n);
 cudaError_t exclusive_scan(cudaStream_t, const uint32_t*, uint32_t*, size_t, uint32_t*);
 cudaError_t radix_sort(cudaStream_t, uint32_t*, uint32_t*, uint32_t*, uint32_t*, size_t, const uint32_t*, int, uint32_t,
-                       uint32_t*, uint32_t*, bool*);
+                       uint32_t*, uint32_t*, bool*, const uint2*, uint32_t, uint2*);
 cudaError_t raster_fwd(cudaStream_t, const ViewBatch&, const FwdArgs&);
 cudaError_t raster_bwd(cudaStream_t, const ViewBatch&, const BwdArgs&);
 bool raster_config_ok(int ts, int ppl);
@@ -146,7 +146,7 @@ void carve_lists(Carver& c, const ViewBatch& b, uint32_t npad, size_t cap, Lists
 // Stage 1: superblock lists of (point, local tile span) in rank order.
 // flags[1] <- tile pairs P, flags[4] <- superblock entries (capacity needed).
 int build_sb_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npad, const uint32_t* order,
-                   const uint2* rect, const ListsWs& L, uint32_t* scan_tmp, uint64_t capacity, uint32_t* flags) {
+                   const uint2* srect, const ListsWs& L, uint32_t* scan_tmp, uint64_t capacity, uint32_t* flags) {
   const uint32_t nchunk = npad / kChunk;
   const size_t m = size_t(b.num_sb) * nchunk;
   const unsigned grid1 = unsigned(b.num_views) * nchunk;
@@ -156,13 +156,13 @@ int build_sb_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npa
     if (smem3 > 200 * 1024) return fail(DSPLAT_ERR_UNSUPPORTED, "too many superblocks in one view");
     TRY_CUDA(cudaFuncSetAttribute(k_sb_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)), "attr");
   }
-  k_sb_count<<<grid1, 256, smem1, st>>>(order, rect, n, npad, b, L.cnt1, flags + 1);
+  k_sb_count<<<grid1, 256, smem1, st>>>(order, srect, n, npad, b, L.cnt1, flags + 1);
   count_launch();
   TRY_CUDA(cudaMemsetAsync(L.cnt1 + m, 0, sizeof(uint32_t), st), "memset");
   TRY_CUDA(exclusive_scan(st, L.cnt1, L.off1, m + 1, scan_tmp), "scan");
   k_copy_total<<<1, 32, 0, st>>>(L.off1, m, flags + 4);
   count_launch();
-  k_sb_scatter<<<grid1, 256, smem3, st>>>(order, rect, n, npad, b, L.off1, capacity, L.list1, flags);
+  k_sb_scatter<<<grid1, 256, smem3, st>>>(order, srect, n, npad, b, L.off1, capacity, L.list1, flags);
   count_launch();
   TRY_CUDA(cudaGetLastError(), "superblock lists");
   return DSPLAT_OK;
@@ -242,6 +242,7 @@ void fill_sb_layout(ViewBatch* b) {
 struct TileWs {
   uint32_t* flags;  // [0] flags, [1] total pairs
   uint2* rect;
+  uint2* srect;  // tile spans in depth order (written by the sort's last pass)
   uint32_t *cnt, *dka, *dva, *dkb, *dvb, *hist, *scan_tmp, *out_tile;
   ListsWs lists;
   size_t bytes;
@@ -271,6 +272,7 @@ TileWs carve_tiles(void* ws, uint32_t n, uint32_t tile_w, uint32_t tile_h, uint6
   TileWs t;
   t.flags = c.take<uint32_t>(16);
   t.rect = c.take<uint2>(n + 1);
+  t.srect = c.take<uint2>(npad);
   t.cnt = c.take<uint32_t>(size_t(n) + 1);
   t.dka = c.take<uint32_t>(npad);
   t.dva = c.take<uint32_t>(npad);
@@ -336,9 +338,11 @@ int tiles_fill(cudaStream_t st, uint32_t n, const float* xyd, const float* aabb,
                                                   t.dka, t.cnt);
   count_launch();
   bool in_b = false;
-  TRY_CUDA(radix_sort(st, t.dka, t.dva, t.dkb, t.dvb, npad, nullptr, 32, 1, t.hist, t.scan_tmp, &in_b), "depth sort");
+  TRY_CUDA(radix_sort(st, t.dka, t.dva, t.dkb, t.dvb, npad, nullptr, 32, 1, t.hist, t.scan_tmp, &in_b, t.rect, n,
+                      t.srect),
+           "depth sort");
   const uint32_t* order = in_b ? t.dvb : t.dva;
-  int rc = build_sb_lists(st, b, n, npad, order, t.rect, t.lists, t.scan_tmp, capacity, t.flags);
+  int rc = build_sb_lists(st, b, n, npad, order, t.srect, t.lists, t.scan_tmp, capacity, t.flags);
   if (rc) return rc;
   rc = build_tile_lists(st, b, npad, t.lists, t.scan_tmp, tile2idx, idx2pnt, keys64 ? t.out_tile : nullptr, capacity,
                         t.flags);
@@ -359,6 +363,7 @@ struct BatchWs {
   uint32_t* flags;
   float4* rec;
   uint2* rect;
+  uint2* srect;  // tile spans in depth order per view (written by the sort's last pass)
   uint32_t *cnt, *dka, *dva, *dkb, *dvb, *hist, *scan_tmp;
   ListsWs lists;
   float* pix_T;
@@ -423,6 +428,7 @@ BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity)
   w.flags = c.take<uint32_t>(16, &L.off_flags);
   w.rec = c.take<float4>(3 * VN + 3, &L.off_rec);
   w.rect = c.take<uint2>(VN + 1, &L.off_rect);
+  w.srect = c.take<uint2>(Vp);
   w.cnt = c.take<uint32_t>(VN + 1, &L.off_cnt);
   w.dka = c.take<uint32_t>(Vp);
   w.dva = c.take<uint32_t>(Vp, &L.off_order);  // 4 passes of 8 bits end back in (dka, dva)
@@ -658,10 +664,12 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
     count_launch();
     stage_mark(st, 1);
     bool in_b = false;
-    TRY_CUDA(radix_sort(st, w.dka, w.dva, w.dkb, w.dvb, Vp, nullptr, 32, V, w.hist, w.scan_tmp, &in_b), "depth sort");
+    TRY_CUDA(radix_sort(st, w.dka, w.dva, w.dkb, w.dvb, Vp, nullptr, 32, V, w.hist, w.scan_tmp, &in_b, w.rect, n,
+                        w.srect),
+             "depth sort");
     stage_mark(st, 2);
     const uint32_t* order = in_b ? w.dvb : w.dva;
-    int rc2 = build_sb_lists(st, b, n, npad, order, w.rect, w.lists, w.scan_tmp, pair_capacity, w.flags);
+    int rc2 = build_sb_lists(st, b, n, npad, order, w.srect, w.lists, w.scan_tmp, pair_capacity, w.flags);
     if (rc2) return rc2;
     stage_mark(st, 3);
   }

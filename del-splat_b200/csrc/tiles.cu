@@ -167,7 +167,8 @@ __global__ void __launch_bounds__(kRsThreads) k_radix_upsweep(const uint32_t* __
 
 __global__ void __launch_bounds__(kRsThreads) k_radix_downsweep(
     const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
-    uint32_t* __restrict__ vout, int shift, uint32_t nb_seg, const uint32_t* __restrict__ offs, int write_keys) {
+    uint32_t* __restrict__ vout, int shift, uint32_t nb_seg, const uint32_t* __restrict__ offs, int write_keys,
+    const uint2* __restrict__ gather_src, uint32_t gather_n, uint2* __restrict__ gather_dst) {
   __shared__ uint32_t wc[kRsWarps][256];
   __shared__ uint32_t dstart[256];
   __shared__ uint32_t goff[256];
@@ -233,8 +234,16 @@ __global__ void __launch_bounds__(kRsThreads) k_radix_downsweep(
     const uint32_t key = sk[i];
     const uint32_t d = (key >> shift) & 255u;
     const uint32_t pos = goff[d] + (uint32_t(i) - dstart[d]);
+    const uint32_t val = sv[i];
     if (write_keys) kout[pos] = key;
-    vout[pos] = sv[i];
+    vout[pos] = val;
+    // optional: the value's record gathered into sorted order (segment-major
+    // source, one row of gather_n records per segment; values >= gather_n
+    // are padding and get an empty record)
+    if (gather_dst) {
+      const uint32_t seg = blockIdx.x / nb_seg;
+      gather_dst[pos] = val < gather_n ? gather_src[size_t(seg) * gather_n + val] : make_uint2(0u, 0u);
+    }
   }
 }
 
@@ -245,9 +254,11 @@ size_t radix_hist_words(size_t n) { return ((n + kRsTile - 1) / kRsTile) * 256; 
 // the keys of the last pass are not written (callers use the values only).
 // n must be a multiple of 4096 (per segment when nseg > 1); count_ptr must be
 // null (every element takes part).
+// gather_dst (nullable): the last pass also writes, per sorted position,
+// gather_src[segment * gather_n + value] (an empty record for padding).
 cudaError_t radix_sort(cudaStream_t st, uint32_t* ka, uint32_t* va, uint32_t* kb, uint32_t* vb, size_t n,
                        const uint32_t* count_ptr, int nbits, uint32_t nseg, uint32_t* hist, uint32_t* scan_tmp,
-                       bool* result_in_b) {
+                       bool* result_in_b, const uint2* gather_src, uint32_t gather_n, uint2* gather_dst) {
   if (n % kRsTile != 0 || count_ptr != nullptr || nseg == 0 || (n / kRsTile) % nseg != 0)
     return cudaErrorInvalidValue;
   const uint32_t nblocks = uint32_t(n / kRsTile);
@@ -267,7 +278,8 @@ cudaError_t radix_sort(cudaStream_t st, uint32_t* ka, uint32_t* va, uint32_t* kb
     cudaError_t e = exclusive_scan(st, hist, hist, hw, scan_tmp);
     if (e != cudaSuccess) return e;
     const int last = shift + 8 >= nbits;
-    k_radix_downsweep<<<nblocks, kRsThreads, 0, st>>>(ki, vi, ko, vo, shift, nb_seg, hist, last ? 0 : 1);
+    k_radix_downsweep<<<nblocks, kRsThreads, 0, st>>>(ki, vi, ko, vo, shift, nb_seg, hist, last ? 0 : 1,
+                                                       gather_src, gather_n, last ? gather_dst : nullptr);
     count_launch();
     in_b = !in_b;
   }
@@ -319,7 +331,7 @@ constexpr int kMsChunk = kMsThreads * kMsRounds;  // 4096 ranks per chunk
 // exclusive scan in index order yields (view, superblock, rank) positions.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restrict__ order,
-                                                         const uint2* __restrict__ rect, uint32_t n, uint32_t npad,
+                                                         const uint2* __restrict__ srect, uint32_t n, uint32_t npad,
                                                          const ViewBatch b,
                                                          uint32_t* __restrict__ cnt,
                                                          uint32_t* __restrict__ total_pairs) {
@@ -334,9 +346,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restr
   const size_t base = size_t(v) * npad + size_t(c) * kMsChunk;
   uint32_t pairs = 0;
   for (int i = threadIdx.x; i < kMsChunk; i += kMsThreads) {
-    const uint32_t g = order[base + i];
-    if (g >= n) continue;
-    const uint2 rc = rect[size_t(v) * n + g];
+    const uint2 rc = srect[base + i];
     int sx0, sy0, sx1, sy1;
     if (!sb_span(rc, sl, &sx0, &sy0, &sx1, &sy1)) continue;
     pairs += uint32_t((rc.y & 0xffff) - (rc.x & 0xffff)) * uint32_t((rc.y >> 16) - (rc.x >> 16));
@@ -360,7 +370,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restr
 // colmask[x] & rowmask[y], and a lane's slot is its popcount among them.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __restrict__ order,
-                                                           const uint2* __restrict__ rect, uint32_t n, uint32_t npad,
+                                                           const uint2* __restrict__ srect, uint32_t n, uint32_t npad,
                                                            const ViewBatch b,
                                                            const uint32_t* __restrict__ off, uint64_t capacity,
                                                            uint2* __restrict__ list1, uint32_t* __restrict__ flags) {
@@ -381,9 +391,8 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
   uint32_t* my = wc + warp * nsb;
   // phase 1: per-warp counts
   for (int r = 0; r < kMsRounds; ++r) {
-    const uint32_t g = order[base + r * 32 + lane];
     int sx0, sy0, sx1, sy1;
-    if (g < n && sb_span(rect[size_t(v) * n + g], sl, &sx0, &sy0, &sx1, &sy1))
+    if (sb_span(srect[base + r * 32 + lane], sl, &sx0, &sy0, &sx1, &sy1))
       for (int sy = sy0; sy < sy1; ++sy)
         for (int sx = sx0; sx < sx1; ++sx) atomicAdd(&my[sy * sbw + sx], 1u);
   }
@@ -403,8 +412,8 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
   for (int r = 0; r < kMsRounds; ++r) {
     const uint32_t g = order[base + r * 32 + lane];
     int sx0 = 0, sy0 = 0, sx1 = 0, sy1 = 0;
-    const uint2 rc = g < n ? rect[size_t(v) * n + g] : make_uint2(0u, 0u);
-    const bool has = g < n && sb_span(rc, sl, &sx0, &sy0, &sx1, &sy1);
+    const uint2 rc = srect[base + r * 32 + lane];
+    const bool has = sb_span(rc, sl, &sx0, &sy0, &sx1, &sy1);
     // the round's column / row coverage masks
     int cx0 = has ? sx0 : 255, cx1 = has ? sx1 : 0, cy0 = has ? sy0 : 255, cy1 = has ? sy1 : 0;
 #pragma unroll
