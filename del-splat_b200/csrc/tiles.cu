@@ -365,8 +365,8 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restr
 // ---------------------------------------------------------------------------
 // Stage 1b: stable scatter of point indices into superblock lists.  Warp w
 // owns ranks [w*512, w*512+512) of the chunk in 16 rounds of 32.  In a round,
-// one ballot per superblock column and per superblock row of the view says
-// which lanes' spans cover it; the lanes covering superblock (x, y) are then
+// each lane sets its bit in a shared mask per superblock column and row its
+// span covers; the lanes covering superblock (x, y) are then
 // colmask[x] & rowmask[y], and a lane's slot is its popcount among them.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __restrict__ order,
@@ -414,22 +414,16 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
     int sx0 = 0, sy0 = 0, sx1 = 0, sy1 = 0;
     const uint2 rc = srect[base + r * 32 + lane];
     const bool has = sb_span(rc, sl, &sx0, &sy0, &sx1, &sy1);
-    // the round's column / row coverage masks
-    int cx0 = has ? sx0 : 255, cx1 = has ? sx1 : 0, cy0 = has ? sy0 : 255, cy1 = has ? sy1 : 0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      cx0 = min(cx0, __shfl_xor_sync(0xffffffffu, cx0, o));
-      cx1 = max(cx1, __shfl_xor_sync(0xffffffffu, cx1, o));
-      cy0 = min(cy0, __shfl_xor_sync(0xffffffffu, cy0, o));
-      cy1 = max(cy1, __shfl_xor_sync(0xffffffffu, cy1, o));
+    // the round's column / row coverage masks: every lane clears, then sets
+    // its bit in, the entries of the columns and rows its span covers
+    if (has) {
+      for (int x = sx0; x < sx1; ++x) colmask[x] = 0u;
+      for (int y = sy0; y < sy1; ++y) rowmask[y] = 0u;
     }
-    for (int x = cx0; x < cx1; ++x) {
-      const uint32_t m = __ballot_sync(0xffffffffu, has && x >= sx0 && x < sx1);
-      if (lane == 0) colmask[x] = m;
-    }
-    for (int y = cy0; y < cy1; ++y) {
-      const uint32_t m = __ballot_sync(0xffffffffu, has && y >= sy0 && y < sy1);
-      if (lane == 0) rowmask[y] = m;
+    __syncwarp();
+    if (has) {
+      for (int x = sx0; x < sx1; ++x) atomicOr(&colmask[x], 1u << lane);
+      for (int y = sy0; y < sy1; ++y) atomicOr(&rowmask[y], 1u << lane);
     }
     __syncwarp();
     for (int sy = sy0; sy < sy1; ++sy) {
