@@ -23,6 +23,8 @@ __global__ void k_project_bwd_geom(uint32_t, const float*, const float*, const f
 __global__ void k_project_bwd_colour(uint32_t, int, const float*, const float*, const ViewBatch, const float4*,
                                      float*, float*);
 __global__ void k_adam(size_t, float*, const float*, float*, float*, float, float, float, float, float, float);
+__global__ void k_pair_cost(const ViewBatch, const uint32_t*, uint32_t*);
+bool raster_bwd_paired(int ts);
 __global__ void k_iota_pad(uint32_t*, uint32_t*, uint32_t, uint32_t, uint32_t);
 __global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*, uint32_t*);
 __global__ void k_sb_scatter(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
@@ -371,7 +373,7 @@ struct BatchWs {
   float* grad_pix;
   float* slab_loss;
   float4* grad2d;
-  uint32_t *sched, *task_order, *task_order_bwd, *item_cost;
+  uint32_t *sched, *task_order, *task_order_bwd, *item_cost, *pair_cost;
 };
 
 int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, int32_t ppl, ViewBatch* b) {
@@ -452,6 +454,7 @@ BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity)
   w.task_order = c.take<uint32_t>(size_t(b.num_items) + 1);
   w.task_order_bwd = c.take<uint32_t>(size_t(b.num_items) + 1);
   w.item_cost = c.take<uint32_t>(size_t(b.num_items) + 1);
+  w.pair_cost = c.take<uint32_t>(size_t(b.num_items) + 1);
   L.total_bytes = align_up(c.off, 256);
   return w;
 }
@@ -714,7 +717,13 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
   TRY_CUDA(cudaMemsetAsync(w.grad2d, 0, 3 * VN * sizeof(float4), st), "memset");
   TRY_CUDA(cudaMemsetAsync(w.flags + 3, 0, sizeof(uint32_t), st), "memset");
   // longest-first order from this forward's measured walks
-  TRY_CUDA(order_tasks(st, b, w.lists.off1, w.L.npad / kChunk, w.item_cost, w.sched, w.task_order_bwd), "task order");
+  const uint32_t* bwd_cost = w.item_cost;
+  if (raster_bwd_paired(b.ts)) {
+    k_pair_cost<<<64, 256, 0, st>>>(b, w.item_cost, w.pair_cost);
+    count_launch();
+    bwd_cost = w.pair_cost;
+  }
+  TRY_CUDA(order_tasks(st, b, w.lists.off1, w.L.npad / kChunk, bwd_cost, w.sched, w.task_order_bwd), "task order");
   stage_mark(st, 7);
   const BwdArgs ba{n,           w.rec,    w.lists.list1,  w.lists.off1, w.L.npad / kChunk, pair_capacity,
                    w.task_order_bwd, w.flags + 3, grad_rgb ? grad_rgb : w.grad_pix, w.pix_T, w.pix_stop, w.grad2d};

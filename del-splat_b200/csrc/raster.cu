@@ -130,6 +130,31 @@ struct SbWalk {  // a superblock list filtered to one tile (ballot compaction ke
   }
 };
 
+// A superblock list filtered to the tiles lx .. lx+nx-1 of one superblock row
+// (the paired backward task): an entry is kept if its span meets any of them.
+struct SbWalkSpan {
+  const uint2* list1;
+  uint32_t lx, ly, nx;
+  template <class Src>
+  __device__ __forceinline__ int stage(const Src& src, Ent* sm, uint32_t pos, bool valid, int lane) const {
+    bool m = false;
+    uint32_t g = 0;
+    if (valid) {
+      const uint2 en = list1[pos];
+      g = en.x;
+      const uint32_t lr = en.y;
+      m = lx < ((lr >> 8) & 15u) && lx + nx > (lr & 15u) && ly >= ((lr >> 4) & 15u) && ly < (lr >> 12);
+    }
+    const uint32_t bal = __ballot_sync(0xffffffffu, m);
+    if (m) {
+      const int slot = __popc(bal & ((1u << lane) - 1u));
+      src.stage(&sm[slot], g);
+      sm[slot].d.z = __uint_as_float(pos);
+    }
+    return __popc(bal);
+  }
+};
+
 // y = k q = (kA dx) dx + (k2B dx + kC dy) dy with the conic terms staged
 // pre-scaled: kadxdx = (kA dx) dx and kb2dx = k2B dx are per entry and lane.
 __device__ __forceinline__ float quad_y(float kC, float dy, float kb2dx, float kadxdx) {
@@ -329,13 +354,31 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
 // reproduce the forward bit for bit (the discrete structure -- boxes, stop
 // positions -- comes from the forward).
 // ---------------------------------------------------------------------------
-template <int TS, int PPL_>
+// PAIR (8x8 tiles): one task covers two horizontally adjacent tiles of one
+// superblock, 16 pixels wide, with twice the pixels per lane, so that the
+// per-entry warp reduction serves twice the pixels.  Even-column tiles lead
+// a pair; the odd-column tasks are empty.  The walk keeps entries whose span
+// meets either tile and every pixel still tests the entry's box, which
+// contains the pixel only if the entry is in that pixel's own tile list, so
+// each pixel sees exactly its tile's entries (and its stop position is a
+// position in the shared superblock list).
+template <int TS, int PPL_, bool PAIR>
+struct BwdGeo {
+  static constexpr int GX = PAIR ? 2 * TS : TS;   // task width in pixels
+  static constexpr int PPL = PAIR ? 2 * PPL_ : PPL_;
+  static constexpr int ROW_STEP = 32 / GX;
+  static constexpr int SLAB_ROWS = ROW_STEP * PPL;
+  static constexpr int SLABS = TS / SLAB_ROWS;
+  static_assert(SLABS * SLAB_ROWS == TS && GX <= 32, "backward task geometry");
+};
+
+template <int TS, int PPL_, bool PAIR>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint2* __restrict__ list1,
     const uint32_t* __restrict__ off1, uint32_t nchunk, uint64_t capacity, const uint32_t* __restrict__ order,
     uint32_t* __restrict__ work_counter, const float* __restrict__ grad_pix, const float* __restrict__ pix_T,
     const uint32_t* __restrict__ pix_last, float4* __restrict__ grad2d) {
-  using G = Geo<TS, PPL_>;
+  using G = BwdGeo<TS, PPL_, PAIR>;
   constexpr int PPL = G::PPL;
   __shared__ Ent sm_all[kRasterWarps][32];
   Ent* sm = sm_all[threadIdx.x >> 5];
@@ -349,8 +392,18 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     const uint32_t item = order[task / G::SLABS], slab = task % G::SLABS;
     const ItemGeo ig = item_geo(b, item, off1, nchunk, capacity);
     const ViewDev& vd = b.v[ig.v];
-    const int ix = ig.px0 + (lane % TS);
-    const int iy0 = ig.py0 + int(slab) * G::SLAB_ROWS + (lane / TS);
+    // tiles of this task: 1, or 2 when the superblock holds the right neighbour
+    uint32_t nx = 1;
+    if (PAIR) {
+      if (vd.sb_log2 > 0) {
+        if (ig.lx & 1u) continue;  // the pair's left tile carries it
+        nx = 2;
+      }
+    }
+    const int col = lane % G::GX;
+    const int ix = ig.px0 + col;
+    const int iy0 = ig.py0 + int(slab) * G::SLAB_ROWS + (lane / G::GX);
+    const bool col_in = col < int(nx) * TS;
     const float fx = float(ix) + 0.5f;
     const uint32_t s = ig.s, e = ig.e;
     // per pixel: T in front of the current entry, S = d . (colour behind it),
@@ -365,7 +418,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
       S[k] = 0.f;
       d0[k] = d1[k] = d2[k] = 0.f;
       last[k] = e;  // outside pixels process nothing
-      if (ix < vd.w && iy < vd.h) {
+      if (col_in && ix < vd.w && iy < vd.h) {
         const size_t p = size_t(vd.pix_base) + size_t(iy) * vd.w + ix;
         Tc[k] = pix_T[p];
         last[k] = pix_last[p];
@@ -378,7 +431,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lo_min = min(lo_min, __shfl_xor_sync(0xffffffffu, lo_min, o));
     PackedSrc src{rec + 3 * size_t(ig.v) * n};
-    SbWalk walk{list1, ig.lx, ig.ly};
+    SbWalkSpan walk{list1, ig.lx, ig.ly, nx};
     float* gv = reinterpret_cast<float*>(grad2d + 3 * size_t(ig.v) * n);
     for (uint32_t lo = max(s, lo_min); lo < e; lo += 32) {
       const int cnt = int(min(32u, e - lo));
@@ -561,10 +614,14 @@ static void launch_fwd(cudaStream_t st, const ViewBatch& b, const FwdArgs& a) {
   count_launch();
 }
 
+// 8x8 tiles run the paired backward (see k_raster_bwd)
+bool raster_bwd_paired(int ts) { return ts == 8; }
+
 template <int TS, int PPL>
 static void launch_bwd(cudaStream_t st, const ViewBatch& b, const BwdArgs& a) {
-  const uint32_t tasks = b.num_items * Geo<TS, PPL>::SLABS;
-  k_raster_bwd<TS, PPL><<<persistent_grid(k_raster_bwd<TS, PPL>, tasks), 32 * kRasterWarps, 0, st>>>(
+  constexpr bool PAIR = TS == 8;
+  const uint32_t tasks = b.num_items * BwdGeo<TS, PPL, PAIR>::SLABS;
+  k_raster_bwd<TS, PPL, PAIR><<<persistent_grid(k_raster_bwd<TS, PPL, PAIR>, tasks), 32 * kRasterWarps, 0, st>>>(
       b, a.n, a.rec, a.list1, a.off1, a.nchunk, a.capacity, a.order, a.counter, a.grad_pix, a.pix_T, a.pix_last,
       a.grad2d);
   count_launch();
