@@ -23,8 +23,8 @@ __global__ void k_project_bwd_geom(uint32_t, const float*, const float*, const f
 __global__ void k_project_bwd_colour(uint32_t, int, const float*, const float*, const ViewBatch, const float4*,
                                      float*, float*);
 __global__ void k_adam(size_t, float*, const float*, float*, float*, float, float, float, float, float, float);
-__global__ void k_pair_cost(const ViewBatch, const uint32_t*, uint32_t*);
-bool raster_bwd_paired(int ts);
+__global__ void k_pair_cost(const ViewBatch, int, const uint32_t*, uint32_t*);
+int raster_bwd_group(int ts);
 __global__ void k_iota_pad(uint32_t*, uint32_t*, uint32_t, uint32_t, uint32_t);
 __global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*, uint32_t*);
 __global__ void k_sb_scatter(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
@@ -718,8 +718,8 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
   TRY_CUDA(cudaMemsetAsync(w.flags + 3, 0, sizeof(uint32_t), st), "memset");
   // longest-first order from this forward's measured walks
   const uint32_t* bwd_cost = w.item_cost;
-  if (raster_bwd_paired(b.ts)) {
-    k_pair_cost<<<64, 256, 0, st>>>(b, w.item_cost, w.pair_cost);
+  if (raster_bwd_group(b.ts) > 1) {
+    k_pair_cost<<<64, 256, 0, st>>>(b, raster_bwd_group(b.ts), w.item_cost, w.pair_cost);
     count_launch();
     bwd_cost = w.pair_cost;
   }

@@ -43,6 +43,7 @@
 namespace dsplat {
 
 constexpr int kRasterWarps = 4;  // warps per CTA (independent tasks)
+constexpr int kBwdGroup8 = 2;    // 8x8 tiles per backward task (4 measured slower: registers, partial overlaps)
 
 struct Ent {  // one staged list entry (64 bytes)
   float4 a;   // px, py, k A, k 2B   (k = -log2(e)/2: exp(-q/2) = 2^(k q))
@@ -362,23 +363,23 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
 // contains the pixel only if the entry is in that pixel's own tile list, so
 // each pixel sees exactly its tile's entries (and its stop position is a
 // position in the shared superblock list).
-template <int TS, int PPL_, bool PAIR>
+template <int TS, int PPL_, int NT>
 struct BwdGeo {
-  static constexpr int GX = PAIR ? 2 * TS : TS;   // task width in pixels
-  static constexpr int PPL = PAIR ? 2 * PPL_ : PPL_;
+  static constexpr int GX = NT * TS;   // task width in pixels
+  static constexpr int PPL = NT * PPL_;
   static constexpr int ROW_STEP = 32 / GX;
   static constexpr int SLAB_ROWS = ROW_STEP * PPL;
   static constexpr int SLABS = TS / SLAB_ROWS;
   static_assert(SLABS * SLAB_ROWS == TS && GX <= 32, "backward task geometry");
 };
 
-template <int TS, int PPL_, bool PAIR>
+template <int TS, int PPL_, int NT>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint2* __restrict__ list1,
     const uint32_t* __restrict__ off1, uint32_t nchunk, uint64_t capacity, const uint32_t* __restrict__ order,
     uint32_t* __restrict__ work_counter, const float* __restrict__ grad_pix, const float* __restrict__ pix_T,
     const uint32_t* __restrict__ pix_last, float4* __restrict__ grad2d) {
-  using G = BwdGeo<TS, PPL_, PAIR>;
+  using G = BwdGeo<TS, PPL_, NT>;
   constexpr int PPL = G::PPL;
   __shared__ Ent sm_all[kRasterWarps][32];
   Ent* sm = sm_all[threadIdx.x >> 5];
@@ -394,11 +395,9 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     const ViewDev& vd = b.v[ig.v];
     // tiles of this task: 1, or 2 when the superblock holds the right neighbour
     uint32_t nx = 1;
-    if (PAIR) {
-      if (vd.sb_log2 > 0) {
-        if (ig.lx & 1u) continue;  // the pair's left tile carries it
-        nx = 2;
-      }
+    if (NT > 1) {
+      nx = min(uint32_t(NT), 1u << vd.sb_log2);
+      if (ig.lx % nx) continue;  // the group's leftmost tile carries it
     }
     const int col = lane % G::GX;
     const int ix = ig.px0 + col;
@@ -614,14 +613,14 @@ static void launch_fwd(cudaStream_t st, const ViewBatch& b, const FwdArgs& a) {
   count_launch();
 }
 
-// 8x8 tiles run the paired backward (see k_raster_bwd)
-bool raster_bwd_paired(int ts) { return ts == 8; }
+// tiles per backward task (see k_raster_bwd): 2 for 8x8 tiles
+int raster_bwd_group(int ts) { return ts == 8 ? kBwdGroup8 : 1; }
 
 template <int TS, int PPL>
 static void launch_bwd(cudaStream_t st, const ViewBatch& b, const BwdArgs& a) {
-  constexpr bool PAIR = TS == 8;
-  const uint32_t tasks = b.num_items * BwdGeo<TS, PPL, PAIR>::SLABS;
-  k_raster_bwd<TS, PPL, PAIR><<<persistent_grid(k_raster_bwd<TS, PPL, PAIR>, tasks), 32 * kRasterWarps, 0, st>>>(
+  constexpr int NT = TS == 8 ? kBwdGroup8 : 1;
+  const uint32_t tasks = b.num_items * BwdGeo<TS, PPL, NT>::SLABS;
+  k_raster_bwd<TS, PPL, NT><<<persistent_grid(k_raster_bwd<TS, PPL, NT>, tasks), 32 * kRasterWarps, 0, st>>>(
       b, a.n, a.rec, a.list1, a.off1, a.nchunk, a.capacity, a.order, a.counter, a.grad_pix, a.pix_T, a.pix_last,
       a.grad2d);
   count_launch();

@@ -618,21 +618,24 @@ __global__ void k_order_scatter(const ViewBatch b, const uint32_t* __restrict__ 
     order[atomicAdd(&sched[40 + item_cost_bucket(b, i, off1, nchunk, cost)], 1u)] = i;
 }
 
-// Costs for the paired backward on 8x8 tiles (two adjacent tiles of a
-// superblock per task): a pair costs the longer of its tiles' walks; the
-// odd-column tiles of superblocks wider than one tile lead no task (cost 1:
+// Costs for the grouped backward (nt adjacent tiles of a superblock row per
+// task, fewer where the superblock is narrower): a group costs the longest
+// of its tiles' walks; the other tiles of a group lead no task (cost 1:
 // ordered among the cheapest; their tasks return at once).
-__global__ void k_pair_cost(const ViewBatch b, const uint32_t* __restrict__ cost, uint32_t* __restrict__ pair_cost) {
+__global__ void k_pair_cost(const ViewBatch b, int nt, const uint32_t* __restrict__ cost,
+                            uint32_t* __restrict__ pair_cost) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.num_items; i += gridDim.x * blockDim.x) {
     int v = 0;
     for (int k = 1; k < b.num_views; ++k)
       if (i >= b.v[k].item_base) v = k;
     const ViewDev& vd = b.v[v];
     const uint32_t tx = (i - vd.item_base) % uint32_t(vd.tile_w);
+    const uint32_t nx = min(uint32_t(nt), 1u << vd.sb_log2);
     uint32_t c = cost[i];
-    if (vd.sb_log2 > 0) {
-      if (tx & 1u) c = 1u;
-      else if (tx + 1 < uint32_t(vd.tile_w)) c = max(c, cost[i + 1]);
+    if (tx % nx) {
+      c = 1u;
+    } else {
+      for (uint32_t k = 1; k < nx && tx + k < uint32_t(vd.tile_w); ++k) c = max(c, cost[i + k]);
     }
     pair_cost[i] = c;
   }
