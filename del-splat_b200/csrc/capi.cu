@@ -25,6 +25,7 @@ __global__ void k_project_bwd_colour(uint32_t, int, const float*, const float*, 
 __global__ void k_adam(size_t, float*, const float*, float*, float*, float, float, float, float, float, float);
 __global__ void k_pair_cost(const ViewBatch, int, const uint32_t*, uint32_t*);
 int raster_bwd_group(int ts);
+int raster_fwd_group(int ts);
 __global__ void k_iota_pad(uint32_t*, uint32_t*, uint32_t, uint32_t, uint32_t);
 __global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*, uint32_t*);
 __global__ void k_sb_scatter(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
@@ -677,7 +678,13 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
     stage_mark(st, 3);
   }
   // longest-first raster task order (costs measured by the previous forward)
-  TRY_CUDA(order_tasks(st, b, w.lists.off1, npad / kChunk, w.item_cost, w.sched, w.task_order), "task order");
+  const uint32_t* fwd_cost = w.item_cost;
+  if (raster_fwd_group(b.ts) > 1) {
+    k_pair_cost<<<64, 256, 0, st>>>(b, raster_fwd_group(b.ts), w.item_cost, w.pair_cost);
+    count_launch();
+    fwd_cost = w.pair_cost;
+  }
+  TRY_CUDA(order_tasks(st, b, w.lists.off1, npad / kChunk, fwd_cost, w.sched, w.task_order), "task order");
   TRY_CUDA(cudaMemsetAsync(w.item_cost, 0, size_t(b.num_items) * sizeof(uint32_t), st), "memset");
   stage_mark(st, 4);
   const FwdArgs fa{n,           w.rec,   w.lists.list1, w.lists.off1, npad / kChunk, pair_capacity, w.task_order,

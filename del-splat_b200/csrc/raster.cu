@@ -43,6 +43,7 @@
 namespace dsplat {
 
 constexpr int kRasterWarps = 4;  // warps per CTA (independent tasks)
+constexpr int kFwdGroup8 = 2;    // 8x8 tiles per forward task
 constexpr int kBwdGroup8 = 2;    // 8x8 tiles per backward task (4 measured slower: registers, partial overlaps)
 
 struct Ent {  // one staged list entry (64 bytes)
@@ -64,6 +65,19 @@ struct Geo {
   static constexpr int SLAB_ROWS = ROW_STEP * PPL;
   static constexpr int SLABS = TS / SLAB_ROWS;    // warp tasks per tile
   static_assert(SLABS * SLAB_ROWS == TS, "slab geometry");
+};
+
+// Fused-path task geometry: NT horizontally adjacent tiles of a superblock
+// row per warp task (NT > 1 for 8x8 tiles, see k_raster_bwd), NT x the
+// pixels per lane.
+template <int TS, int PPL_, int NT>
+struct TaskGeo {
+  static constexpr int GX = NT * TS;   // task width in pixels
+  static constexpr int PPL = NT * PPL_;
+  static constexpr int ROW_STEP = 32 / GX;
+  static constexpr int SLAB_ROWS = ROW_STEP * PPL;
+  static constexpr int SLABS = TS / SLAB_ROWS;
+  static_assert(SLABS * SLAB_ROWS == TS && GX <= 32, "task geometry");
 };
 
 __device__ __forceinline__ void stage_packed(Ent* dst, const float4* __restrict__ rec, uint32_t g) {
@@ -170,7 +184,7 @@ __device__ __forceinline__ float quad_y(float kC, float dy, float kb2dx, float k
 // ---------------------------------------------------------------------------
 template <int TS, int PPL_, class Walk, class Src>
 __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, Ent* sm, uint32_t s, uint32_t e, int px0,
-                                         int py0, int w, int h, bool accumulate, float* __restrict__ out_rgb,
+                                         int py0, int w, int h, int xend, bool accumulate, float* __restrict__ out_rgb,
                                          size_t pix_base, float* __restrict__ out_T, uint32_t* __restrict__ out_last,
                                          const float* __restrict__ target, float* __restrict__ grad_pix,
                                          float* __restrict__ loss_slot) {
@@ -190,7 +204,7 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
     as[k] = 0.f;
     c0[k] = c1[k] = c2[k] = 0.f;
     last[k] = s;
-    if (ix < w && iy < h) {
+    if (ix < xend && iy < h) {
       live |= 1u << k;
       if (accumulate) {
         const size_t p = pix_base + size_t(iy) * w + ix;
@@ -296,14 +310,14 @@ __device__ __forceinline__ ItemGeo item_geo(const ViewBatch& b, uint32_t item, c
 // walking each tile's entries out of its superblock list.
 // slab_loss: one partial L2 loss per task (when target is given).
 // ---------------------------------------------------------------------------
-template <int TS, int PPL>
+template <int TS, int PPL, int NT>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint2* __restrict__ list1,
     const uint32_t* __restrict__ off1, uint32_t nchunk, uint64_t capacity, const uint32_t* __restrict__ order,
     uint32_t* __restrict__ work_counter, float* __restrict__ out_rgb, float* __restrict__ out_T,
     uint32_t* __restrict__ out_last, const float* __restrict__ target, float* __restrict__ grad_pix,
     float* __restrict__ slab_loss, uint32_t* __restrict__ item_cost) {
-  using G = Geo<TS, PPL>;
+  using G = TaskGeo<TS, PPL, NT>;
   __shared__ Ent sm_all[kRasterWarps][32];
   Ent* sm = sm_all[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -316,12 +330,21 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     const uint32_t item = order[task / G::SLABS], slab = task % G::SLABS;
     const ItemGeo ig = item_geo(b, item, off1, nchunk, capacity);
     const ViewDev& vd = b.v[ig.v];
+    // tiles of this task (NT > 1: a run of a superblock row, see k_raster_bwd)
+    uint32_t nx = 1;
+    if (NT > 1) {
+      nx = min(uint32_t(NT), 1u << vd.sb_log2);
+      if (ig.lx % nx) {  // carried by the run's leftmost tile
+        if (target && slab_loss && lane == 0) slab_loss[size_t(item) * G::SLABS + slab] = 0.f;
+        continue;
+      }
+    }
     PackedSrc src{rec + 3 * size_t(ig.v) * n};
-    SbWalk walk{list1, ig.lx, ig.ly};
-    const uint32_t walked =
-        fwd_slab<TS, PPL>(walk, src, sm, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, false,
-                          out_rgb, vd.pix_base, out_T, out_last, target, grad_pix,
-                          slab_loss ? slab_loss + size_t(item) * G::SLABS + slab : nullptr);
+    SbWalkSpan walk{list1, ig.lx, ig.ly, nx};
+    const int xend = min(vd.w, ig.px0 + int(nx) * TS);
+    const uint32_t walked = fwd_slab<G::GX, G::PPL>(
+        walk, src, sm, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, xend, false, out_rgb,
+        vd.pix_base, out_T, out_last, target, grad_pix, slab_loss ? slab_loss + size_t(item) * G::SLABS + slab : nullptr);
     // scheduling hint for the backward and the next forward: list positions walked
     if (lane == 0 && walked) atomicMax(&item_cost[item], walked);
     __syncwarp();
@@ -344,7 +367,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
   const int px0 = int(tile % uint32_t(tile_w)) * TS;
   const int py0 = int(tile / uint32_t(tile_w)) * TS + int(slab) * G::SLAB_ROWS;
   TileWalk walk{idx2pnt};
-  fwd_slab<TS, PPL>(walk, src, sm, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, true, pix2rgb, 0, out_T,
+  fwd_slab<TS, PPL>(walk, src, sm, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, w, true, pix2rgb, 0, out_T,
                     out_last, nullptr, nullptr, nullptr);
 }
 
@@ -355,31 +378,22 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
 // reproduce the forward bit for bit (the discrete structure -- boxes, stop
 // positions -- comes from the forward).
 // ---------------------------------------------------------------------------
-// PAIR (8x8 tiles): one task covers two horizontally adjacent tiles of one
-// superblock, 16 pixels wide, with twice the pixels per lane, so that the
-// per-entry warp reduction serves twice the pixels.  Even-column tiles lead
-// a pair; the odd-column tasks are empty.  The walk keeps entries whose span
-// meets either tile and every pixel still tests the entry's box, which
-// contains the pixel only if the entry is in that pixel's own tile list, so
-// each pixel sees exactly its tile's entries (and its stop position is a
-// position in the shared superblock list).
-template <int TS, int PPL_, int NT>
-struct BwdGeo {
-  static constexpr int GX = NT * TS;   // task width in pixels
-  static constexpr int PPL = NT * PPL_;
-  static constexpr int ROW_STEP = 32 / GX;
-  static constexpr int SLAB_ROWS = ROW_STEP * PPL;
-  static constexpr int SLABS = TS / SLAB_ROWS;
-  static_assert(SLABS * SLAB_ROWS == TS && GX <= 32, "backward task geometry");
-};
-
+// NT > 1 (8x8 tiles): one task covers NT horizontally adjacent tiles of one
+// superblock row (fewer where the superblock is narrower), NT x as wide with
+// NT x the pixels per lane, so that the per-entry warp reduction serves NT x
+// the pixels.  The run's leftmost tile leads the task; the other tiles' tasks
+// are empty.  The walk keeps entries whose span meets any of the tiles and
+// every pixel still tests the entry's box, which contains the pixel only if
+// the entry is in that pixel's own tile list, so each pixel sees exactly its
+// tile's entries (and its stop position is a position in the shared
+// superblock list).  The forward groups tiles the same way.
 template <int TS, int PPL_, int NT>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     const ViewBatch b, uint32_t n, const float4* __restrict__ rec, const uint2* __restrict__ list1,
     const uint32_t* __restrict__ off1, uint32_t nchunk, uint64_t capacity, const uint32_t* __restrict__ order,
     uint32_t* __restrict__ work_counter, const float* __restrict__ grad_pix, const float* __restrict__ pix_T,
     const uint32_t* __restrict__ pix_last, float4* __restrict__ grad2d) {
-  using G = BwdGeo<TS, PPL_, NT>;
+  using G = TaskGeo<TS, PPL_, NT>;
   constexpr int PPL = G::PPL;
   __shared__ Ent sm_all[kRasterWarps][32];
   Ent* sm = sm_all[threadIdx.x >> 5];
@@ -606,8 +620,9 @@ static int persistent_grid(K kernel, uint32_t tasks) {
 
 template <int TS, int PPL>
 static void launch_fwd(cudaStream_t st, const ViewBatch& b, const FwdArgs& a) {
-  const uint32_t tasks = b.num_items * Geo<TS, PPL>::SLABS;
-  k_raster_fwd<TS, PPL><<<persistent_grid(k_raster_fwd<TS, PPL>, tasks), 32 * kRasterWarps, 0, st>>>(
+  constexpr int NT = TS == 8 ? kFwdGroup8 : 1;
+  const uint32_t tasks = b.num_items * TaskGeo<TS, PPL, NT>::SLABS;
+  k_raster_fwd<TS, PPL, NT><<<persistent_grid(k_raster_fwd<TS, PPL, NT>, tasks), 32 * kRasterWarps, 0, st>>>(
       b, a.n, a.rec, a.list1, a.off1, a.nchunk, a.capacity, a.order, a.counter, a.out_rgb, a.out_T, a.out_last,
       a.target, a.grad_pix, a.slab_loss, a.item_cost);
   count_launch();
@@ -615,11 +630,12 @@ static void launch_fwd(cudaStream_t st, const ViewBatch& b, const FwdArgs& a) {
 
 // tiles per backward task (see k_raster_bwd): 2 for 8x8 tiles
 int raster_bwd_group(int ts) { return ts == 8 ? kBwdGroup8 : 1; }
+int raster_fwd_group(int ts) { return ts == 8 ? kFwdGroup8 : 1; }
 
 template <int TS, int PPL>
 static void launch_bwd(cudaStream_t st, const ViewBatch& b, const BwdArgs& a) {
   constexpr int NT = TS == 8 ? kBwdGroup8 : 1;
-  const uint32_t tasks = b.num_items * BwdGeo<TS, PPL, NT>::SLABS;
+  const uint32_t tasks = b.num_items * TaskGeo<TS, PPL, NT>::SLABS;
   k_raster_bwd<TS, PPL, NT><<<persistent_grid(k_raster_bwd<TS, PPL, NT>, tasks), 32 * kRasterWarps, 0, st>>>(
       b, a.n, a.rec, a.list1, a.off1, a.nchunk, a.capacity, a.order, a.counter, a.grad_pix, a.pix_T, a.pix_last,
       a.grad2d);
