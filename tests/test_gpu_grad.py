@@ -81,3 +81,30 @@ def test_gradients_small(orc, dev, sh_deg):
         if not _close(np.array(gp), np.array(fd), scale, 1e-3, 1e-2):
             bad.append(("gpu", k, g, c, gp, fd))
     assert not bad, bad[:8]
+
+
+def test_gradients_config2_scale(orc, dev):
+    """262,144 Gaussians, SH 3, 1280x720, L2 loss against a U[0,1] target:
+    GPU gradients vs FP64 central differences on 64 random parameters of
+    visible Gaussians, and vs the FP64 analytic backward on every parameter."""
+    sc, target = scenes.config2()
+    batch, g_gpu, S = _run(orc, dev, sc, target, ts=16)
+    L, g64 = S.backward()
+    for k in GROUPS:
+        ref = g64[k].reshape(sc.n, -1)
+        scale = np.abs(ref).max()
+        ok = _close(g_gpu[k], ref, scale, 1e-3, 1e-2)
+        assert ok.mean() > 0.999, (k, ok.mean(), np.abs(g_gpu[k] - ref).max(), scale)
+    rng = np.random.default_rng(22)
+    vis = np.unique(batch.tile_lists(0)[1])
+    bad = []
+    for _ in range(64):
+        k = GROUPS[rng.integers(0, len(GROUPS))]
+        g = int(rng.choice(vis))
+        c = int(rng.integers(0, g64[k].reshape(sc.n, -1).shape[1]))
+        fd = S.fd(k, g, c, 1e-4)
+        gp = g_gpu[k][g, c]
+        scale = np.abs(g64[k]).max()
+        if not _close(np.array(gp), np.array(fd), scale, 1e-3, 1e-2):
+            bad.append((k, g, c, gp, fd))
+    assert not bad, bad[:8]
