@@ -566,16 +566,30 @@ def main():
     host_step = dict(host_pinned, target=tgt_pinned)
     feed = HostToDeviceFeed(host_step, dev)
 
+    # one captured step per feed slot (the graph bakes in its slot's buffers)
+    slot_graphs = None
+    if graph is not None:
+        from dsplat.gauss import CapturedStep
+        for sl in feed.slots:  # valid inputs for the capture's warm-up runs
+            for name in params:
+                sl[name].copy_(params[name])
+            sl["target"].copy_(target)
+        slot_graphs = [CapturedStep(batch, {name: sl[name] for name in params}, grads, sl["target"])
+                       for sl in feed.slots]
+
     def run_e2e(steps):
         feed.put(host_step)
         for k in range(steps):
             d = feed.get()
             if k + 1 < steps:
                 feed.put(host_step)
-            p = {name: d[name] for name in params}
-            zero_grads()
-            batch.forward(p, target=d["target"])
-            batch.backward(p, grads)
+            if slot_graphs is not None:
+                slot_graphs[next(i for i, sl in enumerate(feed.slots) if sl is d)].replay()
+            else:
+                p = {name: d[name] for name in params}
+                zero_grads()
+                batch.forward(p, target=d["target"])
+                batch.backward(p, grads)
             loss_host.copy_(batch.slab_loss().sum().reshape(1), non_blocking=True)
             feed.release()
 
