@@ -80,3 +80,70 @@ def test_dlpack_layer_rejects_cpu_tensors():
     with pytest.raises(ValueError):
         L3.circle_splat_from_project_spheres(x, 0.1, torch.zeros(15), (8, 8), torch.zeros((4, 3)),
                                              torch.zeros(4), 0)
+
+
+def test_png_roundtrip_float_u8_and_rgba_u32():
+    from dsplat.image import decode_png, encode_png
+    rng = np.random.default_rng(5)
+    f = rng.uniform(-0.1, 1.1, (7, 11, 3)).astype(np.float32)
+    back = decode_png(encode_png(f))
+    assert np.array_equal(back, np.clip(np.rint(f.astype(np.float64) * 255), 0, 255).astype(np.uint8))
+    u = rng.integers(0, 256, (5, 4, 4), dtype=np.uint8)
+    assert np.array_equal(decode_png(encode_png(u)), u)
+    rgba = rng.integers(0, 2 ** 32, (3, 6), dtype=np.uint64).astype(np.uint32)
+    assert np.array_equal(decode_png(encode_png(rgba)), rgba.view(np.uint8).reshape(3, 6, 4))
+
+
+def _colmap_files(tmp_path):
+    import struct
+    cams = struct.pack("<Q", 2)
+    cams += struct.pack("<iIQQ4d", 1, 1, 640, 480, 500.0, 510.0, 320.5, 239.5)
+    cams += struct.pack("<iIQQ4d", 7, 1, 320, 200, 250.0, 250.0, 160.0, 100.0)
+    imgs = struct.pack("<Q", 2)
+    q0, t0 = (0.9238795, 0.0, 0.3826834, 0.0), (0.1, -0.2, 4.0)
+    imgs += struct.pack("<i4d3di", 3, *q0, *t0, 1) + b"view_a.png\x00" + struct.pack("<Q", 2)
+    imgs += struct.pack("<ddq", 10.5, 20.25, 5) + struct.pack("<ddq", 1.0, 2.0, -1)
+    imgs += struct.pack("<i4d3di", 4, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 3.0, 7) + b"b.jpg\x00" + struct.pack("<Q", 0)
+    pts = struct.pack("<Q", 1) + struct.pack("<Q3d3BdQ", 5, 0.1, 0.2, 0.3, 10, 20, 30, 0.5, 2)
+    pts += struct.pack("<4i", 3, 0, 4, 1)
+    for name, data in (("cameras.bin", cams), ("images.bin", imgs), ("points3D.bin", pts)):
+        (tmp_path / name).write_bytes(data)
+    return tmp_path
+
+
+def test_colmap_binary_model_and_views(tmp_path):
+    from dsplat import colmap
+    d = _colmap_files(tmp_path)
+    cams = colmap.read_cameras(d / "cameras.bin")
+    imgs = colmap.read_images(d / "images.bin")
+    pts = colmap.read_points3d(d / "points3D.bin")
+    assert [c.camera_id for c in cams] == [1, 7] and cams[0].params == (500.0, 510.0, 320.5, 239.5)
+    assert imgs[0].name == "view_a.png" and imgs[1].name == "b.jpg" and imgs[1].camera_id == 7
+    assert np.array_equal(imgs[0].point3d_ids, [5, -1]) and np.allclose(imgs[0].xys, [[10.5, 20.25], [1.0, 2.0]])
+    assert pts[0].point3d_id == 5 and list(pts[0].rgb) == [10, 20, 30] and pts[0].track.tolist() == [[3, 0], [4, 1]]
+    views = colmap.views_from_model(cams, imgs, near=0.5, far=50.0)
+    rng = np.random.default_rng(3)
+    for img, view in zip(imgs, views):
+        cam = next(c for c in cams if c.camera_id == img.camera_id)
+        R = colmap.qvec_to_rotation(img.qvec)
+        M = view.mvp.astype(np.float64).reshape(4, 4).T  # column-major -> row-major
+        # points in front of the camera land on the pinhole pixel, nearer -> larger ndc_z
+        xc = np.c_[rng.uniform(-1, 1, (20, 2)), rng.uniform(1.0, 20.0, 20)]
+        xw = (xc - img.tvec) @ R  # R^T (x_c - t)
+        h = np.c_[xw, np.ones(20)] @ M.T
+        ndc = h[:, :3] / h[:, 3:]
+        fx, fy, cx, cy = cam.params
+        u, v = fx * xc[:, 0] / xc[:, 2] + cx, fy * xc[:, 1] / xc[:, 2] + cy
+        px = 0.5 * cam.width * ndc[:, 0] + 0.5 * cam.width
+        py = -0.5 * cam.height * ndc[:, 1] + 0.5 * cam.height
+        assert np.allclose(px, u, atol=1e-3) and np.allclose(py, v, atol=1e-3)
+        order = np.argsort(xc[:, 2])
+        assert np.all(np.diff(ndc[order, 2]) < 0)
+        assert np.allclose(view.campos, -R.T @ img.tvec, atol=1e-5)
+    # near plane -> +1, far plane -> -1
+    R = colmap.qvec_to_rotation(imgs[1].qvec)
+    M = views[1].mvp.astype(np.float64).reshape(4, 4).T
+    for z, want in ((0.5, 1.0), (50.0, -1.0)):
+        xw = (np.array([0.0, 0.0, z]) - imgs[1].tvec) @ R
+        hh = M @ np.r_[xw, 1.0]
+        assert abs(hh[2] / hh[3] - want) < 1e-6
