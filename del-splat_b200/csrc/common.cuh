@@ -164,6 +164,70 @@ __device__ __forceinline__ float exp2_det(float y) {
   return __int_as_float(int(uint32_t(__float_as_int(p)) + (n << 23)));
 }
 
+// Packed two-wide FP32 (sm_100 f32x2): each element is the exactly rounded
+// IEEE result of the scalar operation, so packed and scalar sequences give
+// the same bits.  f2 holds (lo, hi) = (first, second) element.
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 f2_make(float lo, float hi) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ f2 f2_dup(float v) { return f2_make(v, v); }
+__device__ __forceinline__ float f2_lo(f2 v) {
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+  return lo;
+}
+__device__ __forceinline__ float f2_hi(f2 v) {
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+  return hi;
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+  f2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+  f2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+  f2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+  f2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+// exp2_det on both elements: the fast path runs packed, the (rare) case of
+// an element outside (-125, 123) falls back to the scalar function; every
+// element equals exp2_det of it.
+__device__ __forceinline__ f2 exp2_det2(f2 y) {
+  const float y0 = f2_lo(y), y1 = f2_hi(y);
+  const f2 yp1 = add2(y, f2_dup(1.f));
+  if (!(fabsf(f2_lo(yp1)) < 124.f) || !(fabsf(f2_hi(yp1)) < 124.f)) return f2_make(exp2_det(y0), exp2_det(y1));
+  const f2 magic = f2_dup(12582912.f);
+  const f2 t = add2(y, magic);
+  const f2 f = sub2(y, sub2(t, magic));
+  f2 p = f2_dup(1.5403530393381608e-4f);
+  p = fma2(p, f, f2_dup(1.3333558146428443e-3f));
+  p = fma2(p, f, f2_dup(9.6181291076284772e-3f));
+  p = fma2(p, f, f2_dup(5.5504108664821580e-2f));
+  p = fma2(p, f, f2_dup(2.4022650695910071e-1f));
+  p = fma2(p, f, f2_dup(6.9314718055994531e-1f));
+  p = fma2(p, f, f2_dup(1.f));
+  const uint32_t n0 = uint32_t(__float_as_int(f2_lo(t)) - __float_as_int(12582912.f));
+  const uint32_t n1 = uint32_t(__float_as_int(f2_hi(t)) - __float_as_int(12582912.f));
+  return f2_make(__int_as_float(int(uint32_t(__float_as_int(f2_lo(p))) + (n0 << 23))),
+                 __int_as_float(int(uint32_t(__float_as_int(f2_hi(p))) + (n1 << 23))));
+}
+
 // Hardware approximations (PTX ex2.approx / rcp.approx, flush-to-zero) for
 // the backward, whose values need not reproduce the forward bit for bit.
 __device__ __forceinline__ float ex2_approx(float y) {

@@ -46,12 +46,37 @@ constexpr int kRasterWarps = 4;  // warps per CTA (independent tasks)
 constexpr int kFwdGroup8 = 2;    // 8x8 tiles per forward task
 constexpr int kBwdGroup8 = 2;    // 8x8 tiles per backward task (4 measured slower: registers, partial overlaps)
 
-struct Ent {  // one staged list entry (64 bytes)
+struct Ent {  // one staged list entry (64 bytes), backward
   float4 a;   // px, py, k A, k 2B   (k = -log2(e)/2: exp(-q/2) = 2^(k q))
   float4 b;   // k C, opacity, r, g
   float4 c;   // b, box x0, box y0, box x1
   float4 d;   // box y1, point index (bits), list position (bits), -
+  __device__ __forceinline__ void set_pos(uint32_t pos) { d.z = __uint_as_float(pos); }
 };
+
+// A staged entry for the forward, whose pixel slots are evaluated in pairs
+// with packed two-wide FP32: every value a pair uses is stored twice, so a
+// 64-bit shared load yields the packed operand (96 bytes).
+struct EntP {
+  float4 a;  // px, px, py, py
+  float4 b;  // k A, k A, k 2B, k 2B
+  float4 c;  // k C, k C, opacity, opacity
+  float4 d;  // r, r, g, g
+  float4 e;  // b, b, box x0, box x1
+  float4 f;  // box y0, box y1, point index (bits), list position (bits)
+  __device__ __forceinline__ void set_pos(uint32_t pos) { f.w = __uint_as_float(pos); }
+};
+
+__device__ __forceinline__ void make_entp(EntP* dst, float px, float py, float A, float B, float C, float op, float r,
+                                          float g, float b, float x0, float y0, float x1, float y1, uint32_t idx) {
+  const float kA = fm(A, kNegHalfLog2e), k2B = fm(fa(B, B), kNegHalfLog2e), kC = fm(C, kNegHalfLog2e);
+  dst->a = make_float4(px, px, py, py);
+  dst->b = make_float4(kA, kA, k2B, k2B);
+  dst->c = make_float4(kC, kC, op, op);
+  dst->d = make_float4(r, r, g, g);
+  dst->e = make_float4(b, b, x0, x1);
+  dst->f = make_float4(y0, y1, __uint_as_float(idx), 0.f);
+}
 
 // The staged conic, scaled so that y = k q = kA dx^2 + (k2B dx + kC dy) dy.
 __device__ __forceinline__ float4 scaled_conic_a(float px, float py, float A, float B) {
@@ -92,6 +117,12 @@ __device__ __forceinline__ void stage_packed(Ent* dst, const float4* __restrict_
 
 struct AosSrc {
   const float *xyd, *conic, *aabb, *opacity, *rgb;
+  __device__ __forceinline__ void stage(EntP* dst, uint32_t g) const {
+    const size_t i = g;
+    make_entp(dst, xyd[3 * i], xyd[3 * i + 1], conic[3 * i], conic[3 * i + 1], conic[3 * i + 2], opacity[i],
+              rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2], aabb[4 * i], aabb[4 * i + 1], aabb[4 * i + 2],
+              aabb[4 * i + 3], g);
+  }
   __device__ __forceinline__ void stage(Ent* dst, uint32_t g) const {
     const size_t i = g;
     dst->a = scaled_conic_a(xyd[3 * i], xyd[3 * i + 1], conic[3 * i], conic[3 * i + 1]);
@@ -104,6 +135,13 @@ struct AosSrc {
 struct PackedSrc {
   const float4* rec;
   __device__ __forceinline__ void stage(Ent* dst, uint32_t g) const { stage_packed(dst, rec, g); }
+  __device__ __forceinline__ void stage(EntP* dst, uint32_t g) const {
+    const float4 r0 = __ldg(rec + 3 * size_t(g));
+    const float4 r1 = __ldg(rec + 3 * size_t(g) + 1);
+    const float4 r2 = __ldg(rec + 3 * size_t(g) + 2);
+    make_entp(dst, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, fs(r0.x, r2.y), fs(r0.y, r2.z),
+              fa(r0.x, r2.y), fa(r0.y, r2.z), g);
+  }
 };
 
 // Entry walkers: stage up to 32 entries of the list position range
@@ -112,11 +150,11 @@ struct PackedSrc {
 // return how many were staged.
 struct TileWalk {  // a per-tile list (tile2idx / idx2pnt)
   const uint32_t* idx2pnt;
-  template <class Src>
-  __device__ __forceinline__ int stage(const Src& src, Ent* sm, uint32_t pos, bool valid, int lane) const {
+  template <class Src, class E>
+  __device__ __forceinline__ int stage(const Src& src, E* sm, uint32_t pos, bool valid, int lane) const {
     if (valid) {
       src.stage(&sm[lane], idx2pnt[pos]);
-      sm[lane].d.z = __uint_as_float(pos);
+      sm[lane].set_pos(pos);
     }
     return __popc(__ballot_sync(0xffffffffu, valid));
   }
@@ -125,8 +163,8 @@ struct TileWalk {  // a per-tile list (tile2idx / idx2pnt)
 struct SbWalk {  // a superblock list filtered to one tile (ballot compaction keeps the order)
   const uint2* list1;
   uint32_t lx, ly;  // tile position inside its superblock
-  template <class Src>
-  __device__ __forceinline__ int stage(const Src& src, Ent* sm, uint32_t pos, bool valid, int lane) const {
+  template <class Src, class E>
+  __device__ __forceinline__ int stage(const Src& src, E* sm, uint32_t pos, bool valid, int lane) const {
     bool m = false;
     uint32_t g = 0;
     if (valid) {
@@ -139,7 +177,7 @@ struct SbWalk {  // a superblock list filtered to one tile (ballot compaction ke
     if (m) {
       const int slot = __popc(bal & ((1u << lane) - 1u));
       src.stage(&sm[slot], g);
-      sm[slot].d.z = __uint_as_float(pos);
+      sm[slot].set_pos(pos);
     }
     return __popc(bal);
   }
@@ -150,8 +188,8 @@ struct SbWalk {  // a superblock list filtered to one tile (ballot compaction ke
 struct SbWalkSpan {
   const uint2* list1;
   uint32_t lx, ly, nx;
-  template <class Src>
-  __device__ __forceinline__ int stage(const Src& src, Ent* sm, uint32_t pos, bool valid, int lane) const {
+  template <class Src, class E>
+  __device__ __forceinline__ int stage(const Src& src, E* sm, uint32_t pos, bool valid, int lane) const {
     bool m = false;
     uint32_t g = 0;
     if (valid) {
@@ -164,7 +202,7 @@ struct SbWalkSpan {
     if (m) {
       const int slot = __popc(bal & ((1u << lane) - 1u));
       src.stage(&sm[slot], g);
-      sm[slot].d.z = __uint_as_float(pos);
+      sm[slot].set_pos(pos);
     }
     return __popc(bal);
   }
@@ -183,23 +221,26 @@ __device__ __forceinline__ float quad_y(float kC, float dy, float kb2dx, float k
 // of the time.
 // ---------------------------------------------------------------------------
 template <int TS, int PPL_, class Walk, class Src>
-__device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, Ent* sm, uint32_t s, uint32_t e, int px0,
-                                         int py0, int w, int h, int xend, bool accumulate, float* __restrict__ out_rgb,
-                                         size_t pix_base, float* __restrict__ out_T, uint32_t* __restrict__ out_last,
-                                         const float* __restrict__ target, float* __restrict__ grad_pix,
-                                         float* __restrict__ loss_slot) {
+__device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, EntP* sm, uint32_t s, uint32_t e,
+                                         int px0, int py0, int w, int h, int xend, bool accumulate,
+                                         float* __restrict__ out_rgb, size_t pix_base, float* __restrict__ out_T,
+                                         uint32_t* __restrict__ out_last, const float* __restrict__ target,
+                                         float* __restrict__ grad_pix, float* __restrict__ loss_slot) {
   using G = Geo<TS, PPL_>;
   constexpr int PPL = G::PPL;
+  static_assert(PPL % 2 == 0, "pixel slots are evaluated in pairs");
+  constexpr int NP = PPL / 2;
   const int lane = threadIdx.x & 31;
   const int ix = px0 + (lane % TS);
   const int iy0 = py0 + (lane / TS);
   const float fx = float(ix) + 0.5f;
-  float T[PPL], as[PPL], c0[PPL], c1[PPL], c2[PPL];
+  float T[PPL], as[PPL], c0[PPL], c1[PPL], c2[PPL], fy[PPL];
   uint32_t last[PPL];
   uint32_t live = 0;
 #pragma unroll
   for (int k = 0; k < PPL; ++k) {
     const int iy = iy0 + k * G::ROW_STEP;
+    fy[k] = float(iy) + 0.5f;
     T[k] = 1.f;
     as[k] = 0.f;
     c0[k] = c1[k] = c2[k] = 0.f;
@@ -214,6 +255,18 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
       }
     }
   }
+  // slot pairs (2p, 2p+1) in packed registers during the walk
+  f2 T2[NP], as2[NP], c02[NP], c12[NP], c22[NP], fy2[NP];
+#pragma unroll
+  for (int q = 0; q < NP; ++q) {
+    T2[q] = f2_make(T[2 * q], T[2 * q + 1]);
+    as2[q] = f2_make(as[2 * q], as[2 * q + 1]);
+    c02[q] = f2_make(c0[2 * q], c0[2 * q + 1]);
+    c12[q] = f2_make(c1[2 * q], c1[2 * q + 1]);
+    c22[q] = f2_make(c2[2 * q], c2[2 * q + 1]);
+    fy2[q] = f2_make(fy[2 * q], fy[2 * q + 1]);
+  }
+  const f2 fx2 = f2_dup(fx);
   const uint32_t inside = live;
   uint32_t hi = e;
   while (hi > s) {
@@ -222,29 +275,45 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
     __syncwarp();
     if (live) {
       for (int j = 0; j < k_staged; ++j) {
-        const float4 ea = sm[j].a, eb = sm[j].b, ec = sm[j].c, ed = sm[j].d;
-        if (!(ec.y <= fx && fx <= ec.w)) continue;
-        const float dx = fs(fx, ea.x);
-        const float kadxdx = fm(fm(ea.z, dx), dx);
-        const float kb2dx = fm(ea.w, dx);
-        const uint32_t pos = __float_as_uint(ed.z);
+        const float4 ee = sm[j].e;
+        if (!(ee.z <= fx && fx <= ee.w)) continue;
+        const ulonglong2 qa = *reinterpret_cast<const ulonglong2*>(&sm[j].a);  // (px,px) (py,py)
+        const ulonglong2 qb = *reinterpret_cast<const ulonglong2*>(&sm[j].b);  // (kA,kA) (k2B,k2B)
+        const ulonglong2 qc = *reinterpret_cast<const ulonglong2*>(&sm[j].c);  // (kC,kC) (op,op)
+        const ulonglong2 qd = *reinterpret_cast<const ulonglong2*>(&sm[j].d);  // (r,r) (g,g)
+        const f2 qbl = *reinterpret_cast<const f2*>(&sm[j].e);                  // (b,b)
+        const float4 ef = sm[j].f;
+        const f2 dx2 = sub2(fx2, qa.x);
+        const f2 kadxdx2 = mul2(mul2(qb.x, dx2), dx2);
+        const f2 kb2dx2 = mul2(qb.y, dx2);
+        const uint32_t pos = __float_as_uint(ef.w);
 #pragma unroll
-        for (int k = 0; k < PPL; ++k) {
-          // a slot is one row pair across the warp: the skip is warp-uniform in practice
-          if (!((live >> k) & 1u)) continue;
-          const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
-          if (!(ec.z <= fy && fy <= ed.x)) continue;
-          const float dy = fs(fy, ea.y);
-          const float al = fm(exp2_det(quad_y(eb.x, dy, kb2dx, kadxdx)), eb.y);
-          const float eo = fm(T[k], al);
-          c0[k] = ff(eb.z, eo, c0[k]);
-          c1[k] = ff(eb.w, eo, c1[k]);
-          c2[k] = ff(ec.x, eo, c2[k]);
-          T[k] = fs(T[k], eo);
-          as[k] = fa(as[k], eo);
-          if (as[k] >= kAlphaBreak) {
-            live &= ~(1u << k);
-            last[k] = pos;
+        for (int q = 0; q < NP; ++q) {
+          // a slot is one row of the slab across the warp: the skips are
+          // warp-uniform in practice
+          const int k0 = 2 * q, k1 = 2 * q + 1;
+          const bool a0 = ((live >> k0) & 1u) && ef.x <= fy[k0] && fy[k0] <= ef.y;
+          const bool a1 = ((live >> k1) & 1u) && ef.x <= fy[k1] && fy[k1] <= ef.y;
+          if (!(a0 || a1)) continue;
+          const f2 dy2 = sub2(fy2[q], qa.y);
+          const f2 y2 = fma2(fma2(qc.x, dy2, kb2dx2), dy2, kadxdx2);
+          const f2 ex2v = exp2_det2(y2);
+          // an inactive slot of the pair takes alpha 0: its state is unchanged
+          const f2 e2 = f2_make(a0 ? f2_lo(ex2v) : 0.f, a1 ? f2_hi(ex2v) : 0.f);
+          const f2 al2 = mul2(e2, qc.y);
+          const f2 eo2 = mul2(T2[q], al2);
+          c02[q] = fma2(qd.x, eo2, c02[q]);
+          c12[q] = fma2(qd.y, eo2, c12[q]);
+          c22[q] = fma2(qbl, eo2, c22[q]);
+          T2[q] = sub2(T2[q], eo2);
+          as2[q] = add2(as2[q], eo2);
+          if (a0 && f2_lo(as2[q]) >= kAlphaBreak) {
+            live &= ~(1u << k0);
+            last[k0] = pos;
+          }
+          if (a1 && f2_hi(as2[q]) >= kAlphaBreak) {
+            live &= ~(1u << k1);
+            last[k1] = pos;
           }
         }
         if (!live) break;
@@ -253,6 +322,17 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
     hi -= uint32_t(cnt);
     if (!__any_sync(0xffffffffu, live != 0u)) break;
     __syncwarp();
+  }
+#pragma unroll
+  for (int q = 0; q < NP; ++q) {
+    T[2 * q] = f2_lo(T2[q]);
+    T[2 * q + 1] = f2_hi(T2[q]);
+    c0[2 * q] = f2_lo(c02[q]);
+    c0[2 * q + 1] = f2_hi(c02[q]);
+    c1[2 * q] = f2_lo(c12[q]);
+    c1[2 * q + 1] = f2_hi(c12[q]);
+    c2[2 * q] = f2_lo(c22[q]);
+    c2[2 * q + 1] = f2_hi(c22[q]);
   }
   float l = 0.f;
 #pragma unroll
@@ -318,8 +398,8 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     uint32_t* __restrict__ out_last, const float* __restrict__ target, float* __restrict__ grad_pix,
     float* __restrict__ slab_loss, uint32_t* __restrict__ item_cost) {
   using G = TaskGeo<TS, PPL, NT>;
-  __shared__ Ent sm_all[kRasterWarps][32];
-  Ent* sm = sm_all[threadIdx.x >> 5];
+  __shared__ EntP sm_all[kRasterWarps][32];
+  EntP* sm = sm_all[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const uint32_t num_tasks = b.num_items * G::SLABS;
   for (;;) {
@@ -359,8 +439,8 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
     const uint32_t* __restrict__ tile2idx, const uint32_t* __restrict__ idx2pnt, float* __restrict__ out_T,
     uint32_t* __restrict__ out_last) {
   using G = Geo<TS, PPL>;
-  __shared__ Ent sm_all[kRasterWarps][32];
-  Ent* sm = sm_all[threadIdx.x >> 5];
+  __shared__ EntP sm_all[kRasterWarps][32];
+  EntP* sm = sm_all[threadIdx.x >> 5];
   const uint32_t task = blockIdx.x * kRasterWarps + (threadIdx.x >> 5);
   if (task >= num_tasks) return;
   const uint32_t tile = task / G::SLABS, slab = task % G::SLABS;
