@@ -19,9 +19,10 @@ __global__ void k_prep_tiles(uint32_t, const float*, const float*, const float*,
 __global__ void k_fused_project(uint32_t, uint32_t, int, const float*, const float*, const float*, const float*,
                                 const float*, const ViewBatch, float4*, uint2*, uint32_t*, uint32_t*);
 __global__ void k_project_bwd_geom(uint32_t, const float*, const float*, const float*, const ViewBatch,
-                                   const float4*, float*, float*, float*, float*);
-__global__ void k_project_bwd_colour(uint32_t, int, const float*, const float*, const ViewBatch, const float4*,
-                                     float*, float*);
+                                   float4*, float*, float*, float*, float*);
+__global__ void k_project_bwd_colour(uint32_t, int, const float*, const float*, const ViewBatch, float4*,
+                                     float*, float*, unsigned long long*, unsigned long long);
+__global__ void k_prepare_grad2d(const unsigned long long*, unsigned long long, float4*, size_t);
 __global__ void k_adam(size_t, float*, const float*, float*, float*, float, float, float, float, float, float);
 __global__ void k_pair_cost(const ViewBatch, int, const uint32_t*, uint32_t*);
 int raster_bwd_group(int ts);
@@ -374,6 +375,7 @@ struct BatchWs {
   float* grad_pix;
   float* slab_loss;
   float4* grad2d;
+  unsigned long long* grad2d_tag;  // == grad2d_tag_value(): grad2d is all zero
   uint32_t *sched, *task_order, *task_order_bwd, *item_cost, *pair_cost;
 };
 
@@ -415,6 +417,19 @@ int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, in
   return DSPLAT_OK;
 }
 
+// Value of the workspace's grad2d tag meaning "grad2d is all zero for this
+// layout": a fixed pattern mixed with the layout, so that a fresh workspace
+// or one carved for another batch is cleared before use.
+unsigned long long grad2d_tag_value(const dsplat_batch_layout& L, uint32_t n, int32_t views) {
+  unsigned long long h = 0x6a09e667f3bcc909ull;
+  const unsigned long long parts[4] = {L.total_bytes, L.off_grad2d, n, uint64_t(uint32_t(views))};
+  for (unsigned long long x : parts) {
+    h ^= x + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+    h *= 0xbf58476d1ce4e5b9ull;
+  }
+  return h | 1ull;
+}
+
 BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity) {
   const uint32_t V = uint32_t(b.num_views);
   const uint32_t npad = ceil_div(n > 0 ? n : 1, kSortTile) * kSortTile;
@@ -451,6 +466,7 @@ BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity)
   w.grad_pix = c.take<float>(size_t(b.num_pix) * 3, &L.off_grad_pix);
   w.slab_loss = c.take<float>(size_t(b.num_items) * L.slabs_per_tile, &L.off_slab_loss);
   w.grad2d = c.take<float4>(3 * VN + 3, &L.off_grad2d);
+  w.grad2d_tag = c.take<unsigned long long>(1);
   w.sched = c.take<uint32_t>(80);
   w.task_order = c.take<uint32_t>(size_t(b.num_items) + 1);
   w.task_order_bwd = c.take<uint32_t>(size_t(b.num_items) + 1);
@@ -721,7 +737,12 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t VN = size_t(num_views) * n;
   stage_mark(st, 6);
-  TRY_CUDA(cudaMemsetAsync(w.grad2d, 0, 3 * VN * sizeof(float4), st), "memset");
+  // grad2d must start at zero; the projection backward zeroes what it
+  // consumes, so only a buffer not known to be clean is cleared here
+  const unsigned long long tag = grad2d_tag_value(w.L, n, num_views);
+  k_prepare_grad2d<<<blocks_for(3 * VN, 256) < 4096 ? blocks_for(3 * VN, 256) : 4096, 256, 0, st>>>(
+      w.grad2d_tag, tag, w.grad2d, 3 * VN);
+  count_launch();
   TRY_CUDA(cudaMemsetAsync(w.flags + 3, 0, sizeof(uint32_t), st), "memset");
   // longest-first order from this forward's measured walks
   const uint32_t* bwd_cost = w.item_cost;
@@ -742,7 +763,8 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
                                                          grads->opacity);
   count_launch();
   k_project_bwd_colour<<<blocks_for(n, 128), 128, 0, st>>>(n, params->sh_degree, params->means, params->colors, b,
-                                                           w.grad2d, grads->means, grads->colors);
+                                                           w.grad2d, grads->means, grads->colors, w.grad2d_tag,
+                                                           tag);
   count_launch();
   stage_mark(st, 9);
   TRY_CUDA(cudaGetLastError(), "backward");

@@ -173,7 +173,7 @@ __device__ __forceinline__ void geometry_view(const float* p, const float* dd, c
 __global__ void __launch_bounds__(128) k_project_bwd_geom(uint32_t n, const float* __restrict__ means,
                                                           const float* __restrict__ log_scales,
                                                           const float* __restrict__ quats, const ViewBatch b,
-                                                          const float4* __restrict__ grad2d,
+                                                          float4* __restrict__ grad2d,
                                                           float* __restrict__ g_means, float* __restrict__ g_ls,
                                                           float* __restrict__ g_quats, float* __restrict__ g_op) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -211,6 +211,11 @@ __global__ void __launch_bounds__(128) k_project_bwd_geom(uint32_t n, const floa
       n1 = *reinterpret_cast<const float2*>(gp + 1);
     }
     if (g0.x == 0.f && g0.y == 0.f && g0.z == 0.f && g0.w == 0.f && g1.x == 0.f && g1.y == 0.f) continue;
+    {  // consumed: leave the record's geometry part zero for the next backward
+      float4* gp = grad2d + 3 * (size_t(v) * n + g);
+      gp[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+      *reinterpret_cast<float2*>(gp + 1) = make_float2(0.f, 0.f);
+    }
     float c[16];
     geometry_view(p, dd, R, b.v[v].mvp, float(b.v[v].w), float(b.v[v].h), g0, g1, c);
 #pragma unroll
@@ -257,9 +262,11 @@ __global__ void __launch_bounds__(kColThreads) k_project_bwd_colour(uint32_t n, 
                                                                     const float* __restrict__ means,
                                                                     const float* __restrict__ colors,
                                                                     const ViewBatch b,
-                                                                    const float4* __restrict__ grad2d,
+                                                                    float4* __restrict__ grad2d,
                                                                     float* __restrict__ g_means,
-                                                                    float* __restrict__ g_col) {
+                                                                    float* __restrict__ g_col,
+                                                                    unsigned long long* __restrict__ clean_tag,
+                                                                    unsigned long long tag) {
   __shared__ float rows[kColThreads * kColStride];
   const int K = sh_deg < 0 ? 1 : (sh_deg + 1) * (sh_deg + 1);
   const int C = 3 * K;
@@ -275,7 +282,7 @@ __global__ void __launch_bounds__(kColThreads) k_project_bwd_colour(uint32_t n, 
 #pragma unroll
   for (int j = 0; j < 48; ++j) gcol[j] = 0.f;
   if (live) {
-    const float* gflat = reinterpret_cast<const float*>(grad2d);
+    float* gflat = reinterpret_cast<float*>(grad2d);
     const float p[3] = {means[3 * g], means[3 * g + 1], means[3 * g + 2]};
     float gm[3] = {0.f, 0.f, 0.f};
     const float* r0 = gflat + 12 * size_t(g) + 6;
@@ -289,6 +296,12 @@ __global__ void __launch_bounds__(kColThreads) k_project_bwd_colour(uint32_t n, 
         nd2 = r[2];
       }
       if (dc[0] == 0.f && dc[1] == 0.f && dc[2] == 0.f) continue;
+      {  // consumed: leave the record's colour part zero for the next backward
+        float* r = gflat + 12 * (size_t(v) * n + g) + 6;
+        r[0] = 0.f;
+        r[1] = 0.f;
+        r[2] = 0.f;
+      }
       if (sh_deg < 0) {
         gcol[0] += dc[0];
         gcol[1] += dc[1];
@@ -342,6 +355,18 @@ __global__ void __launch_bounds__(kColThreads) k_project_bwd_colour(uint32_t n, 
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < cnt * uint32_t(C); i += kColThreads)
     g_col[size_t(g0) * C + i] += rows[(i / C) * kColStride + (i % C)];
+  // after this kernel and k_project_bwd_geom every record is zero again
+  if (blockIdx.x == 0 && threadIdx.x == 0) *clean_tag = tag;
+}
+
+// Clears grad2d unless the tag says it is already all zero (the previous
+// backward on this layout consumed it).  Blocks only read the tag; the
+// colour kernel of the same backward writes it.
+__global__ void k_prepare_grad2d(const unsigned long long* __restrict__ clean_tag, unsigned long long tag,
+                                 float4* __restrict__ grad2d, size_t count) {
+  if (*clean_tag == tag) return;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += size_t(gridDim.x) * blockDim.x)
+    grad2d[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // Adam (Kingma & Ba 2015), bias-corrected, in place: config-4 training step.

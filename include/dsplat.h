@@ -198,7 +198,7 @@ typedef struct {
   size_t off_pix_stop;   /* u32[num_pix] sb_list position where the walk stopped */
   size_t off_grad_pix;   /* f32[num_pix*3] dL/dpixel (loss gradient) */
   size_t off_slab_loss;  /* f32[num_items*slabs_per_tile] partial L2 losses */
-  size_t off_grad2d;     /* float4[V*N*3] per-view 2D gradients */
+  size_t off_grad2d;     /* float4[V*N*3] per-view 2D gradients (zero again after each backward) */
   int32_t sb_log2[32];   /* per view: superblock side = 1 << sb_log2 tiles (0..3) */
 } dsplat_batch_layout;
 

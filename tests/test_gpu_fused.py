@@ -131,3 +131,27 @@ def test_autotuner_picks_a_supported_config(dev):
     rep = {}
     ts, ppl = autotune.tune(p, sc.cameras, 0, torch.rand(npix * 3, device=dev), use_cache=False, report=rep)
     assert (ts, ppl) in autotune.CANDIDATES and len(rep["timings_ms"]) == len(autotune.CANDIDATES)
+
+
+def test_repeated_backward_accumulates_exactly_twice(dev):
+    """The projection backward zeroes the per-view 2D gradients it consumes;
+    a second backward of the same forward must see them rebuilt from zero:
+    gradients after two backward calls are twice those after one (the same
+    atomics order is not guaranteed, so the comparison is to 1e-5 relative)."""
+    sc = _scene(3, n=8000, seed=9)
+    p = params_of(sc, dev)
+    batch = GaussBatch(sc.n, sc.cameras, 8, 3, pair_capacity=1 << 18, device=dev, pixels_per_lane=2)
+    batch.ensure_capacity(p)
+    tgt = torch.rand(int(batch.layout.num_pix) * 3, device=dev)
+    batch.forward(p, target=tgt)
+    g1 = {k: torch.zeros_like(v) for k, v in p.items()}
+    batch.backward(p, g1)
+    g2 = {k: torch.zeros_like(v) for k, v in p.items()}
+    batch.backward(p, g2)
+    batch.backward(p, g2)
+    torch.cuda.synchronize(dev)
+    for k in p:
+        a, b = F(g1[k]).astype(np.float64) * 2, F(g2[k]).astype(np.float64)
+        scale = max(np.abs(a).max(), 1e-30)
+        assert np.abs(a - b).max() <= 1e-5 * scale, k
+        assert np.abs(a).max() > 0, k
