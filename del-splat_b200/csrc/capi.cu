@@ -680,7 +680,7 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
     count_launch();
     k_fused_project<<<blocks_for(n, 128), 128, 0, st>>>(n, npad, params->sh_degree, params->means,
                                                         params->log_scales, params->quats, params->opacity,
-                                                        params->colors, b, w.rec, w.rect, w.dka, w.cnt);
+                                                        params->colors, b, w.rec, w.rect, w.dka, nullptr);
     count_launch();
     stage_mark(st, 1);
     bool in_b = false;

@@ -282,7 +282,7 @@ __global__ void k_prep_tiles(uint32_t n, const float* __restrict__ xyd, const fl
 // Fused projection for a batch of views.  One thread per Gaussian reads its
 // parameters once and writes, for every view v:
 //   rec[v*N+g]   3 x float4 = (px, py, A, B) (C, opacity, r, g) (b, hx, hy, ndcz)
-//   rect[v*N+g]  packed tile span, cnt[v*N+g] = #tiles
+//   rect[v*N+g]  packed tile span, cnt[v*N+g] = #tiles (cnt nullable)
 //   dkey[v*Npad+g] depth key bits(max(ndc_z+1,0)); 0xffffffff when no tile
 // sh_deg < 0: colors are RGB [N,3]; else SH coefficients [N,(deg+1)^2,3].
 // ---------------------------------------------------------------------------
@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(128) k_fused_project(
     rec[3 * o_idx + 1] = make_float4(o.conic[2], op, col[0], col[1]);
     rec[3 * o_idx + 2] = make_float4(col[2], o.hx, o.hy, o.ndcz);
     rect[o_idx] = pack_rect(x0, y0, x1, y1);
-    cnt[o_idx] = c;
+    if (cnt) cnt[o_idx] = c;
     dkey[size_t(v) * npad + g] = c ? depth_bits(o.ndcz) : 0xffffffffu;
   }
 }

@@ -186,12 +186,13 @@ __global__ void __launch_bounds__(kRsThreads) k_radix_downsweep(
     k[r] = kin[base + r * 32 + lane];
     v[r] = vin[base + r * 32 + lane];
   }
-  // phase 1: per-warp digit counts
+  // phase 1: per-warp digit counts (the peer masks are kept for phase 3)
+  uint32_t pm[kRsRounds];
 #pragma unroll
   for (int r = 0; r < kRsRounds; ++r) {
     const uint32_t d = (k[r] >> shift) & 255u;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    if (lane == __ffs(peers) - 1) wc[warp][d] += __popc(peers);
+    pm[r] = __match_any_sync(0xffffffffu, d);
+    if (lane == __ffs(pm[r]) - 1) wc[warp][d] += __popc(pm[r]);
     __syncwarp();
   }
   __syncthreads();
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(kRsThreads) k_radix_downsweep(
 #pragma unroll
   for (int r = 0; r < kRsRounds; ++r) {
     const uint32_t d = (k[r] >> shift) & 255u;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t peers = pm[r];
     const uint32_t rb = wc[warp][d];
     __syncwarp();
     if (lane == __ffs(peers) - 1) wc[warp][d] = rb + __popc(peers);

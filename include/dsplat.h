@@ -190,7 +190,7 @@ typedef struct {
   size_t off_flags;      /* u32[16]: [0] flags, [1] tile pairs, [4] superblock entries */
   size_t off_rec;        /* float4[V*N*3] per-view 2D records */
   size_t off_rect;       /* uint2[V*N] tile spans */
-  size_t off_cnt;        /* u32[V*N] tiles per point */
+  size_t off_cnt;        /* u32[V*N] reserved (tiles per point; not written by the batched forward) */
   size_t off_order;      /* u32[V*npad] points in depth order per view */
   size_t off_sb_start;   /* u32[num_sb*sb_chunks+1] superblock list offsets */
   size_t off_sb_list;    /* uint2[capacity] superblock lists */
