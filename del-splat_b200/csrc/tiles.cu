@@ -165,6 +165,17 @@ __global__ void __launch_bounds__(kRsThreads) k_radix_upsweep(const uint32_t* __
   hist[(size_t(seg) * 256 + threadIdx.x) * nb_seg + b] = sum;
 }
 
+// lanes of the warp whose 8-bit digit equals this lane's (one ballot per bit)
+__device__ __forceinline__ uint32_t peers_of_digit(uint32_t d) {
+  uint32_t m = 0xffffffffu;
+#pragma unroll
+  for (int bit = 0; bit < 8; ++bit) {
+    const uint32_t b = __ballot_sync(0xffffffffu, (d >> bit) & 1u);
+    m &= ((d >> bit) & 1u) ? b : ~b;
+  }
+  return m;
+}
+
 __global__ void __launch_bounds__(kRsThreads) k_radix_downsweep(
     const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
     uint32_t* __restrict__ vout, int shift, uint32_t nb_seg, const uint32_t* __restrict__ offs, int write_keys,
@@ -191,7 +202,7 @@ __global__ void __launch_bounds__(kRsThreads) k_radix_downsweep(
 #pragma unroll
   for (int r = 0; r < kRsRounds; ++r) {
     const uint32_t d = (k[r] >> shift) & 255u;
-    pm[r] = __match_any_sync(0xffffffffu, d);
+    pm[r] = peers_of_digit(d);
     if (lane == __ffs(pm[r]) - 1) wc[warp][d] += __popc(pm[r]);
     __syncwarp();
   }
