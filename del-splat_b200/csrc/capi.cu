@@ -194,11 +194,11 @@ cudaError_t order_tasks(cudaStream_t st, const ViewBatch& b, const uint32_t* off
                         const uint32_t* cost, uint32_t* sched, uint32_t* order) {
   cudaError_t e = cudaMemsetAsync(sched, 0, 80 * sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
-  k_order_hist<<<64, 256, 0, st>>>(b, off1, nchunk, cost, sched);
+  k_order_hist<<<296, 256, 0, st>>>(b, off1, nchunk, cost, sched);
   count_launch();
   k_order_scan<<<1, 32, 0, st>>>(sched);
   count_launch();
-  k_order_scatter<<<64, 256, 0, st>>>(b, off1, nchunk, cost, sched, order);
+  k_order_scatter<<<296, 256, 0, st>>>(b, off1, nchunk, cost, sched, order);
   count_launch();
   return cudaGetLastError();
 }

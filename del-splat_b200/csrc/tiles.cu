@@ -623,11 +623,30 @@ __global__ void k_order_scan(uint32_t* __restrict__ sched) {
   }
 }
 
+// Scatter into bucket order: each block ranks its items in shared memory and
+// takes one range per bucket from the global cursors (one global atomic per
+// bucket and block instead of one per item on 33 hot counters).
 __global__ void k_order_scatter(const ViewBatch b, const uint32_t* __restrict__ off1, uint32_t nchunk,
                                 const uint32_t* __restrict__ cost, uint32_t* __restrict__ sched,
                                 uint32_t* __restrict__ order) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.num_items; i += gridDim.x * blockDim.x)
-    order[atomicAdd(&sched[40 + item_cost_bucket(b, i, off1, nchunk, cost)], 1u)] = i;
+  __shared__ uint32_t cnt[33], base[33];
+  const uint32_t per_block = (b.num_items + gridDim.x - 1) / gridDim.x;
+  const uint32_t lo = blockIdx.x * per_block, hi = min(b.num_items, lo + per_block);
+  for (uint32_t i0 = lo; i0 < hi; i0 += blockDim.x) {
+    if (threadIdx.x < 33) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t i = i0 + threadIdx.x;
+    uint32_t bucket = 0, slot = 0;
+    if (i < hi) {
+      bucket = item_cost_bucket(b, i, off1, nchunk, cost);
+      slot = atomicAdd(&cnt[bucket], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 33 && cnt[threadIdx.x]) base[threadIdx.x] = atomicAdd(&sched[40 + threadIdx.x], cnt[threadIdx.x]);
+    __syncthreads();
+    if (i < hi) order[base[bucket] + slot] = i;
+    __syncthreads();
+  }
 }
 
 // Costs for the grouped backward (nt adjacent tiles of a superblock row per
