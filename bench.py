@@ -135,6 +135,15 @@ def dist_setup():
     return rank, world, local
 
 
+def rank_cameras(base, rank: int, views: int):
+    """Weak scaling: every rank renders its own `views` cameras of the same
+    scene (rank 0 the workload's own; rank r > 0 seeded from 1000 + r)."""
+    from dsplat import scenes
+    if rank == 0:
+        return base.cameras
+    return scenes.sphere_cameras(np.random.default_rng(1000 + rank), views, 3.0, scenes.CONFIG3_RESOLUTIONS)
+
+
 def max_over_ranks(x: float, world: int, dev) -> float:
     if world == 1:
         return x
@@ -440,8 +449,7 @@ def main():
     L = _native.lib()
     base = scenes.config3(seed=3, n=args.n, views=args.views, tile_size=args.tile)
     # weak scaling: every rank gets its own cameras of the same scene
-    cams = base.cameras if rank == 0 else scenes.sphere_cameras(np.random.default_rng(1000 + rank), args.views, 3.0,
-                                                              scenes.CONFIG3_RESOLUTIONS)
+    cams = rank_cameras(base, rank, args.views)
     host = {"means": base.means, "log_scales": base.log_scales, "quats": base.quats, "opacity": base.opacity,
             "colors": base.colors.reshape(base.n, -1)}
     params = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in host.items()}
