@@ -31,6 +31,9 @@ __global__ void k_iota_pad(uint32_t*, uint32_t*, uint32_t, uint32_t, uint32_t);
 __global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*, uint32_t*);
 __global__ void k_sb_scatter(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
                              uint64_t, uint2*, uint32_t*);
+__global__ void k_sb_scatter_staged(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
+                                    uint64_t, uint2*, uint32_t*, uint32_t);
+size_t sb_scatter_staged_smem(uint32_t max_sb, uint32_t qcap);
 __global__ void k_tile_count(const uint2*, const uint32_t*, uint32_t, uint64_t, const ViewBatch, uint32_t*);
 __global__ void k_tile_scatter(const uint2*, const uint32_t*, uint32_t, uint64_t, const ViewBatch, const uint32_t*,
                                uint32_t*, uint32_t*, uint32_t*);
@@ -166,7 +169,19 @@ int build_sb_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npa
   TRY_CUDA(exclusive_scan(st, L.cnt1, L.off1, m + 1, scan_tmp), "scan");
   k_copy_total<<<1, 32, 0, st>>>(L.off1, m, flags + 4);
   count_launch();
-  k_sb_scatter<<<grid1, 256, smem3, st>>>(order, srect, n, npad, b, L.off1, capacity, L.list1, flags);
+  // staged scatter (coalesced list stores) when its shared memory fits
+  constexpr uint32_t kStageEntries = 3072;
+  const size_t smem_staged = sb_scatter_staged_smem(b.max_sb, kStageEntries);
+  if (smem_staged <= 100 * 1024) {
+    if (smem_staged > 48 * 1024)
+      TRY_CUDA(cudaFuncSetAttribute(k_sb_scatter_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(smem_staged)),
+               "attr");
+    k_sb_scatter_staged<<<grid1, 256, smem_staged, st>>>(order, srect, n, npad, b, L.off1, capacity, L.list1, flags,
+                                                         kStageEntries);
+  } else {
+    k_sb_scatter<<<grid1, 256, smem3, st>>>(order, srect, n, npad, b, L.off1, capacity, L.list1, flags);
+  }
   count_launch();
   TRY_CUDA(cudaGetLastError(), "superblock lists");
   return DSPLAT_OK;

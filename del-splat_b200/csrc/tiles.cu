@@ -461,6 +461,143 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
 }
 
 // ---------------------------------------------------------------------------
+// Stage 1b, staged: the same result as k_sb_scatter with coalesced stores.
+// The chunk is processed in sub-passes of kSubRanks consecutive ranks (each
+// warp takes kSubRanks / 8 consecutive ranks of the sub-pass).  A sub-pass's
+// entries are ranked per superblock (per-warp counts, one block-wide scan)
+// into a shared-memory stage ordered by superblock, then each superblock's
+// run is written to its contiguous range of the superblock list (the block's
+// cursor for that superblock advances sub-pass by sub-pass).  A sub-pass
+// with more entries than the stage holds writes the same slots directly.
+// Shared memory (words): counters [8][max_sb], cursors [max_sb], stage
+// bases [max_sb + 2] (one spare word keeps the stage 8-byte aligned), masks
+// [8][512], then the stage (uint2[qcap]) and its superblock ids (u16[qcap]).
+// ---------------------------------------------------------------------------
+constexpr int kSubRounds = 2;
+constexpr int kSubRanks = kMsThreads * kSubRounds;  // 512 ranks per sub-pass
+
+size_t sb_scatter_staged_smem(uint32_t max_sb, uint32_t qcap) {
+  return (size_t(kMsWarps) * max_sb + 2 * size_t(max_sb) + 2 + kMsWarps * 512) * 4 + size_t(qcap) * 8 +
+         ((size_t(qcap) + 1) / 2) * 4;
+}
+
+__global__ void __launch_bounds__(kMsThreads) k_sb_scatter_staged(const uint32_t* __restrict__ order,
+                                                                  const uint2* __restrict__ srect, uint32_t n,
+                                                                  uint32_t npad, const ViewBatch b,
+                                                                  const uint32_t* __restrict__ off, uint64_t capacity,
+                                                                  uint2* __restrict__ list1,
+                                                                  uint32_t* __restrict__ flags, uint32_t qcap) {
+  extern __shared__ uint32_t smem_ms[];
+  __shared__ uint32_t sub_total;
+  const uint32_t nchunk = npad / kMsChunk;
+  const uint32_t v = blockIdx.x / nchunk, c = blockIdx.x % nchunk;
+  const ViewDev& vd = b.v[v];
+  const int sl = vd.sb_log2, sbw = sb_cols(vd), sbh = sb_rows(vd);
+  const int nsb = sbw * sbh;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t M = b.max_sb;
+  uint32_t* wc = smem_ms;                     // [kMsWarps][nsb]
+  uint32_t* cur = wc + kMsWarps * M;          // [nsb]
+  uint32_t* sbase = cur + M;                  // [nsb + 1]
+  uint32_t* colmask = sbase + M + 2 + warp * 512;
+  uint32_t* rowmask = colmask + 256;
+  uint2* stage = reinterpret_cast<uint2*>(sbase + M + 2 + kMsWarps * 512);  // 10 M + 4098 words: 8-byte aligned
+  uint16_t* stage_sb = reinterpret_cast<uint16_t*>(stage + qcap);
+  uint32_t* my = wc + warp * nsb;
+  const uint32_t sb0 = vd.sb_base;
+  for (int i = threadIdx.x; i < nsb; i += kMsThreads) cur[i] = off[(size_t(sb0) + i) * nchunk + c];
+  const int seg = (nsb + kMsThreads - 1) / kMsThreads;
+  const int s_lo = min(nsb, int(threadIdx.x) * seg), s_hi = min(nsb, s_lo + seg);
+  for (int sub = 0; sub < kMsChunk / kSubRanks; ++sub) {
+    for (int i = threadIdx.x; i < kMsWarps * nsb; i += kMsThreads) wc[i] = 0;
+    __syncthreads();
+    const size_t base = size_t(v) * npad + size_t(c) * kMsChunk + size_t(sub) * kSubRanks +
+                        size_t(warp) * (kSubRounds * 32);
+    // per-warp counts of the sub-pass
+    for (int r = 0; r < kSubRounds; ++r) {
+      int sx0, sy0, sx1, sy1;
+      if (sb_span(srect[base + r * 32 + lane], sl, &sx0, &sy0, &sx1, &sy1))
+        for (int sy = sy0; sy < sy1; ++sy)
+          for (int sx = sx0; sx < sx1; ++sx) atomicAdd(&my[sy * sbw + sx], 1u);
+    }
+    __syncthreads();
+    // stage layout: superblock-major, then warp (= rank order)
+    uint32_t loc = 0;
+    for (int sb = s_lo; sb < s_hi; ++sb)
+#pragma unroll
+      for (int w = 0; w < kMsWarps; ++w) loc += wc[w * nsb + sb];
+    uint32_t run = block_excl_scan(loc, &sub_total);
+    for (int sb = s_lo; sb < s_hi; ++sb) {
+      sbase[sb] = run;
+#pragma unroll
+      for (int w = 0; w < kMsWarps; ++w) {
+        const uint32_t t = wc[w * nsb + sb];
+        wc[w * nsb + sb] = run;
+        run += t;
+      }
+    }
+    if (threadIdx.x == 0) sbase[nsb] = sub_total;
+    __syncthreads();
+    const uint32_t total = sub_total;
+    const bool staged = total <= qcap;
+    for (int r = 0; r < kSubRounds; ++r) {
+      const uint32_t g = order[base + r * 32 + lane];
+      int sx0 = 0, sy0 = 0, sx1 = 0, sy1 = 0;
+      const uint2 rc = srect[base + r * 32 + lane];
+      const bool has = sb_span(rc, sl, &sx0, &sy0, &sx1, &sy1);
+      if (has) {
+        for (int x = sx0; x < sx1; ++x) colmask[x] = 0u;
+        for (int y = sy0; y < sy1; ++y) rowmask[y] = 0u;
+      }
+      __syncwarp();
+      if (has) {
+        for (int x = sx0; x < sx1; ++x) atomicOr(&colmask[x], 1u << lane);
+        for (int y = sy0; y < sy1; ++y) atomicOr(&rowmask[y], 1u << lane);
+      }
+      __syncwarp();
+      for (int sy = sy0; sy < sy1; ++sy) {
+        const uint32_t rm = rowmask[sy];
+        for (int sx = sx0; sx < sx1; ++sx) {
+          const int sb = sy * sbw + sx;
+          const uint32_t sp = my[sb] + uint32_t(__popc(colmask[sx] & rm & lt));
+          const uint2 en = make_uint2(g, local_rect(rc, sl, sx, sy));
+          if (staged) {
+            stage[sp] = en;
+            stage_sb[sp] = uint16_t(sb);
+          } else {
+            const uint64_t dst = uint64_t(cur[sb]) + (sp - sbase[sb]);
+            if (dst < capacity) list1[dst] = en;
+            else set_flag(flags, kFlagPairOverflow);
+          }
+        }
+      }
+      __syncwarp();
+      for (int sy = sy0; sy < sy1; ++sy) {
+        const uint32_t rm = rowmask[sy];
+        for (int sx = sx0; sx < sx1; ++sx) {
+          const uint32_t m = colmask[sx] & rm;
+          if ((m >> lane) == 1u) my[sy * sbw + sx] += uint32_t(__popc(m));
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    if (staged) {
+      for (uint32_t i = threadIdx.x; i < total; i += kMsThreads) {
+        const int sb = stage_sb[i];
+        const uint64_t dst = uint64_t(cur[sb]) + (i - sbase[sb]);
+        if (dst < capacity) list1[dst] = stage[i];
+        else set_flag(flags, kFlagPairOverflow);
+      }
+    }
+    __syncthreads();
+    for (int sb = threadIdx.x; sb < nsb; sb += kMsThreads) cur[sb] += sbase[sb + 1] - sbase[sb];
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Stage 2a: per-tile pair counts, one CTA per superblock walking its list.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int view_of_sb(const ViewBatch& b, uint32_t sb) {
