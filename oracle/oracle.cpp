@@ -30,6 +30,7 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <parallel/algorithm>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -500,10 +501,16 @@ extern "C" void orc_tile2pnt_fill(int64_t n, const float* aabb,
                                   uint32_t* idx2pnt, uint64_t* keys) {
   const int64_t T = int64_t(tile_w) * tile_h;
   const uint64_t P = tile2idx[T];
-  std::vector<uint64_t> k;
-  std::vector<uint32_t> v;
-  k.reserve(P);
-  v.reserve(P);
+  // (key, point) pairs in emission order; a point appears at most once per
+  // tile and is emitted in index order, so the reference's stable sort by
+  // key equals a sort by (key, point), done here in parallel
+  struct KV {
+    uint64_t k;
+    uint32_t v;
+    bool operator<(const KV& o) const { return k < o.k || (k == o.k && v < o.v); }
+  };
+  std::vector<KV> kv;
+  kv.reserve(P);
   for (int64_t i = 0; i < n; ++i) {
     int x0, y0, x1, y1;
     tile_span(aabb + 4 * i, tile_w, tile_h, ts, &x0, &y0, &x1, &y1);
@@ -511,17 +518,13 @@ extern "C" void orc_tile2pnt_fill(int64_t n, const float* aabb,
     for (int ix = x0; ix < x1; ++ix)
       for (int iy = y0; iy < y1; ++iy) {
         uint64_t tile = uint64_t(iy) * tile_w + ix;
-        k.push_back((tile << 32) | zb);
-        v.push_back(uint32_t(i));
+        kv.push_back(KV{(tile << 32) | zb, uint32_t(i)});
       }
   }
-  std::vector<uint64_t> ord(k.size());
-  std::iota(ord.begin(), ord.end(), 0);
-  std::stable_sort(ord.begin(), ord.end(),
-                   [&](uint64_t a, uint64_t b) { return k[a] < k[b]; });
-  for (uint64_t j = 0; j < ord.size() && j < P; ++j) {
-    idx2pnt[j] = v[ord[j]];
-    if (keys) keys[j] = k[ord[j]];
+  __gnu_parallel::sort(kv.begin(), kv.end());
+  for (uint64_t j = 0; j < kv.size() && j < P; ++j) {
+    idx2pnt[j] = kv[j].v;
+    if (keys) keys[j] = kv[j].k;
   }
 }
 
