@@ -340,9 +340,11 @@ __global__ void __launch_bounds__(128) k_fused_project(
     if (y1 < y0) y1 = y0;
     const uint32_t c = uint32_t(x1 - x0) * uint32_t(y1 - y0);
     const size_t o_idx = size_t(v) * n + g;
-    rec[3 * o_idx + 0] = make_float4(o.px, o.py, o.conic[0], o.conic[1]);
-    rec[3 * o_idx + 1] = make_float4(o.conic[2], op, col[0], col[1]);
-    rec[3 * o_idx + 2] = make_float4(col[2], o.hx, o.hy, o.ndcz);
+    if (c) {  // only points with tiles are ever read back (list entries)
+      rec[3 * o_idx + 0] = make_float4(o.px, o.py, o.conic[0], o.conic[1]);
+      rec[3 * o_idx + 1] = make_float4(o.conic[2], op, col[0], col[1]);
+      rec[3 * o_idx + 2] = make_float4(col[2], o.hx, o.hy, o.ndcz);
+    }
     rect[o_idx] = pack_rect(x0, y0, x1, y1);
     if (cnt) cnt[o_idx] = c;
     dkey[size_t(v) * npad + g] = c ? depth_bits(o.ndcz) : 0xffffffffu;

@@ -200,6 +200,8 @@ class GaussBatch:
             self.num_views, self.n, 12)
 
     def records(self) -> torch.Tensor:
+        """[V, N, 12] per-view 2D records of the last forward; rows of points
+        whose tile span in that view is empty are not written."""
         return self._ws(self.layout.off_rec, self.num_views * self.n * 12, torch.float32).view(
             self.num_views, self.n, 12)
 

@@ -188,7 +188,7 @@ typedef struct {
   uint32_t num_sb;    /* superblocks over all views */
   uint32_t sb_chunks; /* entries of sb_start per superblock */
   size_t off_flags;      /* u32[16]: [0] flags, [1] tile pairs, [4] superblock entries */
-  size_t off_rec;        /* float4[V*N*3] per-view 2D records */
+  size_t off_rec;        /* float4[V*N*3] per-view 2D records (written where the tile span is not empty) */
   size_t off_rect;       /* uint2[V*N] tile spans */
   size_t off_cnt;        /* u32[V*N] reserved (tiles per point; not written by the batched forward) */
   size_t off_order;      /* u32[V*npad] points in depth order per view */
