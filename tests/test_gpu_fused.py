@@ -160,3 +160,23 @@ def test_repeated_backward_accumulates_exactly_twice(dev):
         scale = max(np.abs(a).max(), 1e-30)
         assert np.abs(a - b).max() <= 1e-5 * scale, k
         assert np.abs(a).max() > 0, k
+
+
+def test_large_splats_take_the_direct_scatter_path(orc, dev):
+    """Splats whose boxes span dozens of superblocks give sub-passes with more
+    list entries than the superblock scatter stages in shared memory; those
+    write their entries directly.  Lists, images and stops stay bit-exact."""
+    rng = np.random.default_rng(17)
+    sc = scenes.config0(seed=17, n=3000, size=(64, 64))
+    sc.log_scales = rng.uniform(-1.6, -1.0, (sc.n, 3)).astype(np.float32)  # boxes of ~100-300 px
+    sc.cameras = [scenes.Camera.look_at_origin((0.2, -0.1, -3.0), 512, 512),
+                  scenes.Camera.look_at_origin((1.5, 2.0, 1.5), 384, 256)]
+    p = params_of(sc, dev)
+    batch = GaussBatch(sc.n, sc.cameras, 8, sc.sh_degree, pair_capacity=1 << 20, device=dev, pixels_per_lane=2)
+    batch.ensure_capacity(p)
+    _, needed, _ = batch.status()
+    # 3000 points = 6 sub-passes of 512 ranks per view: on average each holds
+    # more list entries than the 3072 the scatter stages
+    assert needed > len(sc.cameras) * 6 * 3072
+    for v in range(len(sc.cameras)):
+        _check_view(orc, batch, sc, v, 8)
