@@ -56,3 +56,44 @@ def test_layout_grows_with_capacity_and_views():
     L.dsplat_gauss_batch_layout(10000, 1, v, 16, 0, 1 << 16, ctypes.byref(a))
     L.dsplat_gauss_batch_layout(10000, 2, v, 16, 0, 1 << 20, ctypes.byref(b))
     assert b.total_bytes > a.total_bytes and b.num_items == 2 * a.num_items
+
+
+def _sb_rule(tile_w, tile_h, min_per_view=200, max_per_view=4096):
+    """The superblock side rule: the largest side (8 tiles at most) that still
+    splits the view into >= min_per_view superblocks, within 255 superblocks
+    per side and max_per_view per view."""
+    s = 3
+    while s > 0:
+        cw, ch = -(-tile_w // (1 << s)), -(-tile_h // (1 << s))
+        if cw * ch >= min_per_view:
+            break
+        nw, nh = -(-tile_w // (1 << (s - 1))), -(-tile_h // (1 << (s - 1)))
+        if nw > 255 or nh > 255 or nw * nh > max_per_view:
+            break
+        s -= 1
+    return s
+
+
+@pytest.mark.parametrize("ts", [8, 16, 32])
+def test_superblock_side_per_view_follows_the_rule(ts):
+    L = N.lib()
+    sizes = [(320, 240), (640, 480), (1280, 720), (1920, 1080), (64, 64), (16000, 8), (4096, 4096), (1, 1)]
+    v = (N.View * len(sizes))()
+    for i, (w, h) in enumerate(sizes):
+        v[i].width, v[i].height = w, h
+    lay = N.BatchLayout()
+    assert L.dsplat_gauss_batch_layout(5000, len(sizes), v, ts, 0, 1 << 16, ctypes.byref(lay)) == 0
+    total_sb = 0
+    for i, (w, h) in enumerate(sizes):
+        tw, th = -(-w // ts), -(-h // ts)
+        s = _sb_rule(tw, th)
+        assert lay.sb_log2[i] == s, (w, h, ts, lay.sb_log2[i], s)
+        total_sb += -(-tw // (1 << s)) * -(-th // (1 << s))
+    assert lay.num_sb == total_sb
+    # the bench's views at 8x8 tiles: 1, 2, 3, 3 (64-pixel superblocks at 720p/1080p)
+    if ts == 8:
+        assert list(lay.sb_log2[:4]) == [1, 2, 3, 3]
+        # more than 255 superblocks of 8 tiles in a row is rejected
+        v[5].width = 16384
+        assert L.dsplat_gauss_batch_layout(5000, len(sizes), v, ts, 0, 1 << 16, ctypes.byref(lay)) == 5
+        assert b"superblocks" in L.dsplat_last_error()
