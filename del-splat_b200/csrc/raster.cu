@@ -6,19 +6,21 @@
 // e = exp(-q/2) * opacity with q = d^T conic d; rgb += c*T*e; T *= 1-e;
 // alpha_sum += T*e; stop once alpha_sum > 0.999.
 //
-// B200 structure: the unit of work is a warp task = one slab of 256 pixels
-// of one (view, tile) item (a 16x16 tile, a 32x8 quarter of a 32x32 tile or
-// a whole 8x8 tile); each lane owns 8 pixels of one column (2 for 8x8 tiles).
-// A warp stages 32 list entries at a time into its own shared-memory slots
-// (one coalesced index load + one 48-byte record gather per lane), then every
-// lane walks them with 128-bit broadcast reads, amortising each read over its
-// pixels.  The fused path reads each tile's entries straight out of its
-// superblock list (1-8 tiles per side, see tiles.cu): a ballot over the 32 fetched
-// entries keeps those whose tile span covers the tile, compacted in order, so
-// no per-tile list is ever materialised.  The warp stops fetching as soon as all its pixels terminated
-// (__any_sync), so no CTA-wide barrier exists anywhere.  Warps pull tasks
-// from a global counter (work stealing): one persistent launch covers views
-// of different resolutions.
+// B200 structure: the unit of work is a warp task.  With 8x8 tiles a task
+// covers two horizontally adjacent tiles of one superblock (16x8 pixels, 4
+// per lane); with 16x16 or 32x32 tiles a slab of one tile (32 lanes x 2..8
+// pixels).  A lane's pixels share its column.  A warp stages 32 list entries
+// at a time into its own shared-memory slots (one coalesced index load + one
+// 48-byte record gather per lane), then every lane walks them with 128-bit
+// broadcast reads, amortising each read over its pixels.  The fused path
+// reads the entries straight out of the superblock list (1-8 tiles per
+// side, see tiles.cu): a ballot over the 32 fetched entries keeps those whose
+// tile span meets the task's tiles, compacted in order, so no per-tile list
+// is ever materialised.  The forward evaluates a lane's pixels in pairs with
+// packed f32x2 arithmetic.  A forward warp stops fetching as soon as all its
+// pixels terminated (__any_sync), so no CTA-wide barrier exists anywhere.
+// Warps pull tasks from a global counter (work stealing), longest first: one
+// persistent launch covers views of different resolutions.
 //
 // The blend arithmetic is a fixed sequence of exactly rounded IEEE
 // operations (multiply, add, fused multiply-add) with exp(-q/2) evaluated by
@@ -123,13 +125,6 @@ struct AosSrc {
               rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2], aabb[4 * i], aabb[4 * i + 1], aabb[4 * i + 2],
               aabb[4 * i + 3], g);
   }
-  __device__ __forceinline__ void stage(Ent* dst, uint32_t g) const {
-    const size_t i = g;
-    dst->a = scaled_conic_a(xyd[3 * i], xyd[3 * i + 1], conic[3 * i], conic[3 * i + 1]);
-    dst->b = make_float4(fm(conic[3 * i + 2], kNegHalfLog2e), opacity[i], rgb[3 * i], rgb[3 * i + 1]);
-    dst->c = make_float4(rgb[3 * i + 2], aabb[4 * i], aabb[4 * i + 1], aabb[4 * i + 2]);
-    dst->d = make_float4(aabb[4 * i + 3], __uint_as_float(g), 0.f, 0.f);
-  }
 };
 
 struct PackedSrc {
@@ -146,7 +141,7 @@ struct PackedSrc {
 
 // Entry walkers: stage up to 32 entries of the list position range
 // [pos0 - 32, pos0) (backwards) or [pos0, pos0 + 32) (forwards) into the
-// warp's slots, in walk order, with each entry's list position in d.z;
+// warp's slots, in walk order, each with its list position (set_pos);
 // return how many were staged.
 struct TileWalk {  // a per-tile list (tile2idx / idx2pnt)
   const uint32_t* idx2pnt;
@@ -160,31 +155,9 @@ struct TileWalk {  // a per-tile list (tile2idx / idx2pnt)
   }
 };
 
-struct SbWalk {  // a superblock list filtered to one tile (ballot compaction keeps the order)
-  const uint2* list1;
-  uint32_t lx, ly;  // tile position inside its superblock
-  template <class Src, class E>
-  __device__ __forceinline__ int stage(const Src& src, E* sm, uint32_t pos, bool valid, int lane) const {
-    bool m = false;
-    uint32_t g = 0;
-    if (valid) {
-      const uint2 en = list1[pos];
-      g = en.x;
-      const uint32_t lr = en.y;
-      m = lx >= (lr & 15u) && lx < ((lr >> 8) & 15u) && ly >= ((lr >> 4) & 15u) && ly < (lr >> 12);
-    }
-    const uint32_t bal = __ballot_sync(0xffffffffu, m);
-    if (m) {
-      const int slot = __popc(bal & ((1u << lane) - 1u));
-      src.stage(&sm[slot], g);
-      sm[slot].set_pos(pos);
-    }
-    return __popc(bal);
-  }
-};
-
 // A superblock list filtered to the tiles lx .. lx+nx-1 of one superblock row
-// (the paired backward task): an entry is kept if its span meets any of them.
+// (a fused-path warp task): an entry is kept if its span meets any of them;
+// ballot compaction keeps the list order.
 struct SbWalkSpan {
   const uint2* list1;
   uint32_t lx, ly, nx;
