@@ -254,12 +254,16 @@ __device__ __forceinline__ uint32_t depth_bits(float ndcz) {
 
 // tile_acceleration.h:22-31: [floor(min/ts), floor(max/ts)+1) clipped to the
 // tile grid.  Out-of-range and NaN values clamp instead of overflowing.
-__device__ __forceinline__ int tile_lo(float a, float tsf, int lim) {
-  const float f = floorf(__fdiv_rn(a, tsf));
+// Tile sizes are powers of two (8, 16, 32), so a / ts is computed exactly as
+// a * (1 / ts): the same correctly rounded value without a division
+// (inv_ts = tile_inv(ts)).
+__device__ __forceinline__ float tile_inv(int ts) { return ts == 8 ? 0.125f : ts == 16 ? 0.0625f : 0.03125f; }
+__device__ __forceinline__ int tile_lo(float a, float inv_ts, int lim) {
+  const float f = floorf(__fmul_rn(a, inv_ts));
   return (f >= 0.f) ? (f < float(lim) ? int(f) : lim) : 0;
 }
-__device__ __forceinline__ int tile_hi(float a, float tsf, int lim) {
-  const float f = floorf(__fdiv_rn(a, tsf));
+__device__ __forceinline__ int tile_hi(float a, float inv_ts, int lim) {
+  const float f = floorf(__fmul_rn(a, inv_ts));
   return (f >= 0.f) ? (f < float(lim) ? int(f) + 1 : lim) : 0;
 }
 

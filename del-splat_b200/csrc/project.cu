@@ -267,7 +267,7 @@ __global__ void k_prep_tiles(uint32_t n, const float* __restrict__ xyd, const fl
     a2 = x + r;
     a3 = y + r;
   }
-  const float tsf = float(ts);
+  const float tsf = tile_inv(ts);
   int x0 = tile_lo(a0, tsf, tile_w), y0 = tile_lo(a1, tsf, tile_h);
   int x1 = tile_hi(a2, tsf, tile_w), y1 = tile_hi(a3, tsf, tile_h);
   if (x1 < x0) x1 = x0;
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(128) k_fused_project(
 #pragma unroll
   for (int k = 0; k < 48; ++k)
     if (k < 3 * K) coef[k] = colors[size_t(g) * 3 * K + k];
-  const float tsf = float(b.ts);
+  const float tsf = tile_inv(b.ts);
   for (int v = 0; v < b.num_views; ++v) {
     const ViewDev& vd = b.v[v];
     Proj o;

@@ -81,7 +81,7 @@ __global__ void k_circle_zbuf(uint32_t n, const float* __restrict__ xyd, const f
   if (i >= n) return;
   const float x = xyd[3 * i], y = xyd[3 * i + 1], r = rad[i];
   const int tile_w = (w + ts - 1) / ts, tile_h = (h + ts - 1) / ts;
-  const float tsf = float(ts);
+  const float tsf = tile_inv(ts);
   // the circle's tile span, exactly as the tile lists compute it
   const int tx0 = tile_lo(fs(x, r), tsf, tile_w), ty0 = tile_lo(fs(y, r), tsf, tile_h);
   const int tx1 = tile_hi(fa(x, r), tsf, tile_w), ty1 = tile_hi(fa(y, r), tsf, tile_h);
