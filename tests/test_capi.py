@@ -97,3 +97,22 @@ def test_superblock_side_per_view_follows_the_rule(ts):
         v[5].width = 16384
         assert L.dsplat_gauss_batch_layout(5000, len(sizes), v, ts, 0, 1 << 16, ctypes.byref(lay)) == 5
         assert b"superblocks" in L.dsplat_last_error()
+
+
+def test_plain_c_client_builds_and_runs(tmp_path):
+    """The header and library are usable from C alone (the boundary a Rust or
+    C host binds): compile tests/c_abi_smoke.c with gcc, link libdsplat.so."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    exe = tmp_path / "c_abi_smoke"
+    libdir = os.path.dirname(N.LIB_PATH)
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "c_abi_smoke.c"), "-L", libdir, "-ldsplat",
+                        "-Wl,-rpath," + libdir, "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert run.returncode == 0, run.stdout + run.stderr
+    assert "sm_100a" in run.stdout and "rejected" in run.stdout
