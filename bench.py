@@ -40,25 +40,66 @@ UNIT = "views/s"
 
 # --------------------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi sampling during the timed region (SM clock, throttle reasons)."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region.  NVML is polled every `period_s` from a thread of this process,
+    so even a region of ~100 ms gets tens of samples; without NVML,
+    `nvidia-smi -lms 200` runs beside the region instead.  Only reads the
+    GPU's state."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits (nvml.h nvmlClocksEventReason*)
+    REASON_BITS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+                   0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, gpu_index: int):
-        self.idx = gpu_index
+    def __init__(self, device: int, period_s: float = 0.005):
+        self.dev = device
+        self.period = period_s
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []  # (sm MHz, max sm MHz, reason bits)
+        self.stop = threading.Event()
+        self.source = None
+
+    def _bus_id(self):
+        pr = torch.cuda.get_device_properties(self.dev)
+        return f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+
+    def _start_nvml(self):
+        import pynvml
+        pynvml.nvmlInit()
+        h = pynvml.nvmlDeviceGetHandleByPciBusId(self._bus_id())
+        mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+
+        def poll():
+            while True:
+                self.samples.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), mx, int(get_reasons(h))))
+                if self.stop.wait(self.period):
+                    return
+
+        self.nvml = pynvml
+        self.t = threading.Thread(target=poll, daemon=True)
+        self.t.start()
+        self.source = "nvml"
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+            self._start_nvml()
+            return self
+        except Exception:  # no NVML on this host: fall back to nvidia-smi
+            self.nvml = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self._bus_id(), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
-        except OSError:
+            self.source = "nvidia-smi"
+        except (OSError, RuntimeError, AssertionError):
             self.proc = None
         return self
 
@@ -67,6 +108,13 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        if self.nvml is not None:
+            self.stop.set()
+            self.t.join(timeout=2)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -77,6 +125,10 @@ class ClockSampler:
 
     def summary(self):
         sm, mx, reasons = [], None, set()
+        for clk, cmax, bits in self.samples:
+            sm.append(float(clk))
+            mx = float(cmax)
+            reasons.update(name for bit, name in self.REASON_BITS.items() if bits & bit)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.lines:
             parts = [p.strip() for p in line.split(",")]
@@ -91,7 +143,7 @@ class ClockSampler:
                 if val.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": self.source}
 
 
 # --------------------------------------------------------------------------- helpers
