@@ -205,13 +205,10 @@ __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
   return r;
 }
 
-// exp2_det on both elements: the fast path runs packed, the (rare) case of
-// an element outside (-125, 123) falls back to the scalar function; every
-// element equals exp2_det of it.
-__device__ __forceinline__ f2 exp2_det2(f2 y) {
-  const float y0 = f2_lo(y), y1 = f2_hi(y);
-  const f2 yp1 = add2(y, f2_dup(1.f));
-  if (!(fabsf(f2_lo(yp1)) < 124.f) || !(fabsf(f2_hi(yp1)) < 124.f)) return f2_make(exp2_det(y0), exp2_det(y1));
+// exp2_det2_inrange: exp2_det's fast path on both elements, packed; equal
+// to exp2_det for elements in (-125, 123).  A caller that has bounded y to
+// that range (see fwd_slab) uses it directly.
+__device__ __forceinline__ f2 exp2_det2_inrange(f2 y) {
   const f2 magic = f2_dup(12582912.f);
   const f2 t = add2(y, magic);
   const f2 f = sub2(y, sub2(t, magic));
@@ -226,6 +223,15 @@ __device__ __forceinline__ f2 exp2_det2(f2 y) {
   const uint32_t n1 = uint32_t(__float_as_int(f2_hi(t)) - __float_as_int(12582912.f));
   return f2_make(__int_as_float(int(uint32_t(__float_as_int(f2_lo(p))) + (n0 << 23))),
                  __int_as_float(int(uint32_t(__float_as_int(f2_hi(p))) + (n1 << 23))));
+}
+// exp2_det on both elements: the fast path runs packed, the (rare) case of
+// an element outside (-125, 123) falls back to the scalar function; every
+// element equals exp2_det of it.
+__device__ __forceinline__ f2 exp2_det2(f2 y) {
+  const float y0 = f2_lo(y), y1 = f2_hi(y);
+  const f2 yp1 = add2(y, f2_dup(1.f));
+  if (!(fabsf(f2_lo(yp1)) < 124.f) || !(fabsf(f2_hi(yp1)) < 124.f)) return f2_make(exp2_det(y0), exp2_det(y1));
+  return exp2_det2_inrange(y);
 }
 
 // Hardware approximations (PTX ex2.approx / rcp.approx, flush-to-zero) for

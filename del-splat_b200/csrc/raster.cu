@@ -17,7 +17,9 @@
 // side, see tiles.cu): a ballot over the 32 fetched entries keeps those whose
 // tile span meets the task's tiles, compacted in order, so no per-tile list
 // is ever materialised.  The forward evaluates a lane's pixels in pairs with
-// packed f32x2 arithmetic.  A forward warp stops fetching as soon as all its
+// packed f32x2 arithmetic; an entry whose exponent is bounded over its whole
+// box at staging skips exp2_det's range check (the same bits, fewer
+// instructions).  A forward warp stops fetching as soon as all its
 // pixels terminated (__any_sync), so no CTA-wide barrier exists anywhere.
 // Warps pull tasks from a global counter (work stealing), longest first: one
 // persistent launch covers views of different resolutions.
@@ -40,6 +42,8 @@
 // transposed butterfly (9 + 5 shuffles instead of 45), and nine lanes add
 // the finished 2D gradient to the per-(view, point) record with one atomic
 // instruction.
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace dsplat {
@@ -65,19 +69,26 @@ struct EntP {
   float4 c;  // k C, k C, opacity, opacity
   float4 d;  // r, r, g, g
   float4 e;  // b, b, box x0, box x1
-  float4 f;  // box y0, box y1, point index (bits), list position (bits)
+  float4 f;  // box y0, box y1, exponent in range (0/1 bits), list position (bits)
   __device__ __forceinline__ void set_pos(uint32_t pos) { f.w = __uint_as_float(pos); }
 };
 
 __device__ __forceinline__ void make_entp(EntP* dst, float px, float py, float A, float B, float C, float op, float r,
-                                          float g, float b, float x0, float y0, float x1, float y1, uint32_t idx) {
+                                          float g, float b, float x0, float y0, float x1, float y1) {
   const float kA = fm(A, kNegHalfLog2e), k2B = fm(fa(B, B), kNegHalfLog2e), kC = fm(C, kNegHalfLog2e);
+  // The exponent y = kA dx^2 + k2B dx dy + kC dy^2 of every pixel centre in
+  // the box is bounded in magnitude by the same sum of absolute terms at the
+  // box's farthest corner; below 100 (rounding adds far less than the margin
+  // to 123) exp2_det's range check can be skipped for this entry.  NaN or
+  // infinite terms fail the test.
+  const float dxm = fmaxf(fabsf(x0 - px), fabsf(x1 - px)), dym = fmaxf(fabsf(y0 - py), fabsf(y1 - py));
+  const float mag = fabsf(kA) * dxm * dxm + fabsf(k2B) * dxm * dym + fabsf(kC) * dym * dym;
   dst->a = make_float4(px, px, py, py);
   dst->b = make_float4(kA, kA, k2B, k2B);
   dst->c = make_float4(kC, kC, op, op);
   dst->d = make_float4(r, r, g, g);
   dst->e = make_float4(b, b, x0, x1);
-  dst->f = make_float4(y0, y1, __uint_as_float(idx), 0.f);
+  dst->f = make_float4(y0, y1, __uint_as_float(mag < 100.f ? 1u : 0u), 0.f);
 }
 
 // The staged conic, scaled so that y = k q = kA dx^2 + (k2B dx + kC dy) dy.
@@ -123,7 +134,7 @@ struct AosSrc {
     const size_t i = g;
     make_entp(dst, xyd[3 * i], xyd[3 * i + 1], conic[3 * i], conic[3 * i + 1], conic[3 * i + 2], opacity[i],
               rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2], aabb[4 * i], aabb[4 * i + 1], aabb[4 * i + 2],
-              aabb[4 * i + 3], g);
+              aabb[4 * i + 3]);
   }
 };
 
@@ -135,7 +146,7 @@ struct PackedSrc {
     const float4 r1 = __ldg(rec + 3 * size_t(g) + 1);
     const float4 r2 = __ldg(rec + 3 * size_t(g) + 2);
     make_entp(dst, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, fs(r0.x, r2.y), fs(r0.y, r2.z),
-              fa(r0.x, r2.y), fa(r0.y, r2.z), g);
+              fa(r0.x, r2.y), fa(r0.y, r2.z));
   }
 };
 
@@ -260,35 +271,43 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
         const f2 kadxdx2 = mul2(mul2(qb.x, dx2), dx2);
         const f2 kb2dx2 = mul2(qb.y, dx2);
         const uint32_t pos = __float_as_uint(ef.w);
+        // both instances compute the same bits; the first one skips the
+        // exponent range check, which the entry's staged flag has proven
+        auto blend_slots = [&](auto inrange) {
 #pragma unroll
-        for (int q = 0; q < NP; ++q) {
-          // a slot is one row of the slab across the warp: the skips are
-          // warp-uniform in practice
-          const int k0 = 2 * q, k1 = 2 * q + 1;
-          const bool a0 = ((live >> k0) & 1u) && ef.x <= fy[k0] && fy[k0] <= ef.y;
-          const bool a1 = ((live >> k1) & 1u) && ef.x <= fy[k1] && fy[k1] <= ef.y;
-          if (!(a0 || a1)) continue;
-          const f2 dy2 = sub2(fy2[q], qa.y);
-          const f2 y2 = fma2(fma2(qc.x, dy2, kb2dx2), dy2, kadxdx2);
-          const f2 ex2v = exp2_det2(y2);
-          // an inactive slot of the pair takes alpha 0: its state is unchanged
-          const f2 e2 = f2_make(a0 ? f2_lo(ex2v) : 0.f, a1 ? f2_hi(ex2v) : 0.f);
-          const f2 al2 = mul2(e2, qc.y);
-          const f2 eo2 = mul2(T2[q], al2);
-          c02[q] = fma2(qd.x, eo2, c02[q]);
-          c12[q] = fma2(qd.y, eo2, c12[q]);
-          c22[q] = fma2(qbl, eo2, c22[q]);
-          T2[q] = sub2(T2[q], eo2);
-          as2[q] = add2(as2[q], eo2);
-          if (a0 && f2_lo(as2[q]) >= kAlphaBreak) {
-            live &= ~(1u << k0);
-            last[k0] = pos;
+          for (int q = 0; q < NP; ++q) {
+            // a slot is one row of the slab across the warp: the skips are
+            // warp-uniform in practice
+            const int k0 = 2 * q, k1 = 2 * q + 1;
+            const bool a0 = ((live >> k0) & 1u) && ef.x <= fy[k0] && fy[k0] <= ef.y;
+            const bool a1 = ((live >> k1) & 1u) && ef.x <= fy[k1] && fy[k1] <= ef.y;
+            if (!(a0 || a1)) continue;
+            const f2 dy2 = sub2(fy2[q], qa.y);
+            const f2 y2 = fma2(fma2(qc.x, dy2, kb2dx2), dy2, kadxdx2);
+            const f2 ex2v = decltype(inrange)::value ? exp2_det2_inrange(y2) : exp2_det2(y2);
+            // an inactive slot of the pair takes alpha 0: its state is unchanged
+            const f2 e2 = f2_make(a0 ? f2_lo(ex2v) : 0.f, a1 ? f2_hi(ex2v) : 0.f);
+            const f2 al2 = mul2(e2, qc.y);
+            const f2 eo2 = mul2(T2[q], al2);
+            c02[q] = fma2(qd.x, eo2, c02[q]);
+            c12[q] = fma2(qd.y, eo2, c12[q]);
+            c22[q] = fma2(qbl, eo2, c22[q]);
+            T2[q] = sub2(T2[q], eo2);
+            as2[q] = add2(as2[q], eo2);
+            if (a0 && f2_lo(as2[q]) >= kAlphaBreak) {
+              live &= ~(1u << k0);
+              last[k0] = pos;
+            }
+            if (a1 && f2_hi(as2[q]) >= kAlphaBreak) {
+              live &= ~(1u << k1);
+              last[k1] = pos;
+            }
           }
-          if (a1 && f2_hi(as2[q]) >= kAlphaBreak) {
-            live &= ~(1u << k1);
-            last[k1] = pos;
-          }
-        }
+        };
+        if (__float_as_uint(ef.z))
+          blend_slots(std::true_type{});
+        else
+          blend_slots(std::false_type{});
         if (!live) break;
       }
     }
