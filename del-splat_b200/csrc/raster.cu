@@ -18,9 +18,11 @@
 // tile span meets the task's tiles, compacted in order, so no per-tile list
 // is ever materialised.  The forward evaluates a lane's pixels in pairs with
 // packed f32x2 arithmetic; an entry whose exponent is bounded over its whole
-// box at staging skips exp2_det's range check (the same bits, fewer
-// instructions).  A forward warp stops fetching as soon as all its
-// pixels terminated (__any_sync), so no CTA-wide barrier exists anywhere.
+// box at staging skips exp2_det's range check, and one whose box holds every
+// row of the slab skips the per-slot row test (the same bits, fewer
+// instructions; the backward measured slower with the row hoist).  A forward
+// warp stops fetching as soon as all its pixels terminated (__any_sync), so
+// no CTA-wide barrier exists anywhere.
 // Warps pull tasks from a global counter (work stealing), longest first: one
 // persistent launch covers views of different resolutions.
 //
@@ -251,6 +253,8 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
     fy2[q] = f2_make(fy[2 * q], fy[2 * q + 1]);
   }
   const f2 fx2 = f2_dup(fx);
+  // centres of the slab's first and last rows (the same for every lane)
+  const float fy_first = float(py0) + 0.5f, fy_last = float(py0 + G::SLAB_ROWS - 1) + 0.5f;
   const uint32_t inside = live;
   uint32_t hi = e;
   while (hi > s) {
@@ -271,16 +275,17 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
         const f2 kadxdx2 = mul2(mul2(qb.x, dx2), dx2);
         const f2 kb2dx2 = mul2(qb.y, dx2);
         const uint32_t pos = __float_as_uint(ef.w);
-        // both instances compute the same bits; the first one skips the
-        // exponent range check, which the entry's staged flag has proven
-        auto blend_slots = [&](auto inrange) {
+        // all instances compute the same bits: `inrange` skips the exponent
+        // range check (proven by the entry's staged flag), `rows` the row
+        // test of an entry whose box holds every row of the slab
+        auto blend_slots = [&](auto inrange, auto rows) {
 #pragma unroll
           for (int q = 0; q < NP; ++q) {
             // a slot is one row of the slab across the warp: the skips are
             // warp-uniform in practice
             const int k0 = 2 * q, k1 = 2 * q + 1;
-            const bool a0 = ((live >> k0) & 1u) && ef.x <= fy[k0] && fy[k0] <= ef.y;
-            const bool a1 = ((live >> k1) & 1u) && ef.x <= fy[k1] && fy[k1] <= ef.y;
+            const bool a0 = ((live >> k0) & 1u) && (decltype(rows)::value || (ef.x <= fy[k0] && fy[k0] <= ef.y));
+            const bool a1 = ((live >> k1) & 1u) && (decltype(rows)::value || (ef.x <= fy[k1] && fy[k1] <= ef.y));
             if (!(a0 || a1)) continue;
             const f2 dy2 = sub2(fy2[q], qa.y);
             const f2 y2 = fma2(fma2(qc.x, dy2, kb2dx2), dy2, kadxdx2);
@@ -304,10 +309,18 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
             }
           }
         };
-        if (__float_as_uint(ef.z))
-          blend_slots(std::true_type{});
-        else
-          blend_slots(std::false_type{});
+        const bool all_rows = ef.x <= fy_first && fy_last <= ef.y;
+        if (__float_as_uint(ef.z)) {
+          if (all_rows)
+            blend_slots(std::true_type{}, std::true_type{});
+          else
+            blend_slots(std::true_type{}, std::false_type{});
+        } else {
+          if (all_rows)
+            blend_slots(std::false_type{}, std::true_type{});
+          else
+            blend_slots(std::false_type{}, std::false_type{});
+        }
         if (!live) break;
       }
     }
