@@ -101,6 +101,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "orc_fused_project": (None, [_i64, _f32p, _f32p, _f32p, _f32p, _int, _f32p, _f32p, _int, _int,
                                      _f32p, _f32p, _f32p, _f32p]),
         "orc_sh_eval": (None, [_i64, _f32p, _f32p, _int, _f32p, _f32p]),
+        "orc_exp2_det": (None, [_i64, _f32p, _f32p]),
         "orc64_loss": (ctypes.c_double, [ctypes.POINTER(Scene64), _u8p, _f64p]),
         "orc64_backward": (ctypes.c_double, [ctypes.POINTER(Scene64), _f64p, _f64p, _f64p, _f64p, _f64p]),
         "orc64_fd": (ctypes.c_double, [ctypes.POINTER(Scene64), _int, _i64, _int, ctypes.c_double]),
@@ -121,6 +122,14 @@ def _p(a: Optional[np.ndarray], ct):
 
 def f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def exp2_det(y):
+    """The blend's deterministic 2^y (exp2_det), elementwise."""
+    y = f32(y).ravel()
+    out = np.empty_like(y)
+    lib().orc_exp2_det(y.size, _p(y, _f32p), _p(out, _f32p))
+    return out
 
 
 def tile_shape(w: int, h: int, ts: int):

@@ -246,9 +246,9 @@ inline float dexp_f32(float x) {
 // Deterministic 2^y, identical operation for operation to the CUDA
 // exp2_det(): y = n + f with n the nearest integer (adding 1.5 * 2^23 rounds
 // y where the float spacing is 1; n is read from the sum's bits), |f| <= 1/2,
-// the degree-6 Taylor polynomial of e^(f ln 2) in Horner form with fused
-// multiply-adds (std::fma is exactly rounded, like the GPU's fma), and exact
-// scaling by 2^n through the exponent field.  Outside (-125, 123): 0 below,
+// the degree-5 minimax polynomial of 2^f (coefficients from fit_exp2.py) in
+// Horner form with fused multiply-adds (std::fma is exactly rounded, like
+// the GPU's fma), and exact scaling by 2^n through the exponent field.  Outside (-125, 123): 0 below,
 // +inf above, NaN stays NaN.
 inline float exp2_det_f32(float y) {
   if (!(std::fabs(y + 1.f) < 124.f)) {
@@ -257,12 +257,11 @@ inline float exp2_det_f32(float y) {
   }
   const float t = y + 12582912.f;
   const float f = y - (t - 12582912.f);
-  float p = 1.5403530393381608e-4f;
-  p = std::fma(p, f, 1.3333558146428443e-3f);
-  p = std::fma(p, f, 9.6181291076284772e-3f);
-  p = std::fma(p, f, 5.5504108664821580e-2f);
-  p = std::fma(p, f, 2.4022650695910071e-1f);
-  p = std::fma(p, f, 6.9314718055994531e-1f);
+  float p = 0.0013202981790527701f;
+  p = std::fma(p, f, 0.009674952365458012f);
+  p = std::fma(p, f, 0.055510472506284714f);
+  p = std::fma(p, f, 0.24022166430950165f);
+  p = std::fma(p, f, 0.6931465864181519f);
   p = std::fma(p, f, 1.f);
   uint32_t tb, pb, magic;
   const float m = 12582912.f;
@@ -406,6 +405,11 @@ inline void eval_color(int sh_deg, const T* mean, const T* campos,
 }
 
 }  // namespace
+
+// The deterministic 2^y of the blend, elementwise (accuracy tests).
+extern "C" void orc_exp2_det(int64_t n, const float* y, float* out) {
+  for (int64_t i = 0; i < n; ++i) out[i] = exp2_det_f32(y[i]);
+}
 
 // ============================================================================
 // Reference forward path (FP32)
