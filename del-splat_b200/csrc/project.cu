@@ -286,13 +286,26 @@ __global__ void k_prep_tiles(uint32_t n, const float* __restrict__ xyd, const fl
 //   dkey[v*Npad+g] depth key bits(max(ndc_z+1,0)); 0xffffffff when no tile
 // sh_deg < 0: colors are RGB [N,3]; else SH coefficients [N,(deg+1)^2,3].
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_fused_project(
+constexpr int kProjThreads = 128;
+constexpr int kProjStride = 49;  // 48 coefficients + 1 pad (odd stride: conflict-free rows)
+
+__global__ void __launch_bounds__(kProjThreads) k_fused_project(
     uint32_t n, uint32_t npad, int sh_deg, const float* __restrict__ means,
     const float* __restrict__ log_scales, const float* __restrict__ quats,
     const float* __restrict__ opacity, const float* __restrict__ colors, const ViewBatch b,
     float4* __restrict__ rec, uint2* __restrict__ rect, uint32_t* __restrict__ dkey,
     uint32_t* __restrict__ cnt) {
-  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  // the block's colour rows (128 Gaussians x 3K floats, contiguous) are
+  // loaded coalesced into shared memory, padded to an odd stride
+  __shared__ float crow[kProjThreads * kProjStride];
+  const int K = sh_deg < 0 ? 1 : (sh_deg + 1) * (sh_deg + 1);
+  const int C = 3 * K;
+  const uint32_t g0 = blockIdx.x * kProjThreads;
+  const uint32_t cnt_blk = n > g0 ? min(uint32_t(kProjThreads), n - g0) : 0u;
+  for (uint32_t i = threadIdx.x; i < cnt_blk * uint32_t(C); i += kProjThreads)
+    crow[(i / C) * kProjStride + (i % C)] = colors[size_t(g0) * C + i];
+  __syncthreads();
+  const uint32_t g = g0 + threadIdx.x;
   if (g >= n) return;
   const float p[3] = {means[3 * g], means[3 * g + 1], means[3 * g + 2]};
   const float s[3] = {dexp(log_scales[3 * g]), dexp(log_scales[3 * g + 1]),
@@ -303,11 +316,7 @@ __global__ void __launch_bounds__(128) k_fused_project(
   float r[9];
   quat_to_mat3(qn, r);
   const float op = opacity[g];
-  const int K = sh_deg < 0 ? 1 : (sh_deg + 1) * (sh_deg + 1);
-  float coef[48];
-#pragma unroll
-  for (int k = 0; k < 48; ++k)
-    if (k < 3 * K) coef[k] = colors[size_t(g) * 3 * K + k];
+  const float* coef = crow + threadIdx.x * kProjStride;  // read per view from shared memory
   const float tsf = tile_inv(b.ts);
   for (int v = 0; v < b.num_views; ++v) {
     const ViewDev& vd = b.v[v];
