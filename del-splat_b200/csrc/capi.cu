@@ -3,6 +3,7 @@
 // Host orchestration only: argument checks, workspace carving and the launch
 // sequence of each entry point.  No device memory is allocated here; every
 // buffer comes from the caller.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -33,7 +34,7 @@ __global__ void k_sb_scatter(const uint32_t*, const uint2*, uint32_t, uint32_t, 
                              uint64_t, uint2*, uint32_t*);
 __global__ void k_sb_scatter_staged(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
                                     uint64_t, uint2*, uint32_t*, uint32_t);
-size_t sb_scatter_staged_smem(uint32_t max_sb, uint32_t qcap);
+size_t sb_scatter_staged_smem(uint32_t max_sb, uint32_t max_side, uint32_t qcap);
 __global__ void k_tile_count(const uint2*, const uint32_t*, uint32_t, uint64_t, const ViewBatch, uint32_t*);
 __global__ void k_tile_scatter(const uint2*, const uint32_t*, uint32_t, uint64_t, const ViewBatch, const uint32_t*,
                                uint32_t*, uint32_t*, uint32_t*);
@@ -158,7 +159,7 @@ int build_sb_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npa
   const size_t m = size_t(b.num_sb) * nchunk;
   const unsigned grid1 = unsigned(b.num_views) * nchunk;
   const size_t smem1 = size_t(b.max_sb) * sizeof(uint32_t);
-  const size_t smem3 = 8 * smem1 + 8 * 512 * sizeof(uint32_t);
+  const size_t smem3 = 8 * smem1 + 8 * 2 * size_t(b.max_sb_side) * sizeof(uint32_t);
   if (smem3 > 48 * 1024) {
     if (smem3 > 200 * 1024) return fail(DSPLAT_ERR_UNSUPPORTED, "too many superblocks in one view");
     TRY_CUDA(cudaFuncSetAttribute(k_sb_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)), "attr");
@@ -171,7 +172,7 @@ int build_sb_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npa
   count_launch();
   // staged scatter (coalesced list stores) when its shared memory fits
   constexpr uint32_t kStageEntries = 3072;
-  const size_t smem_staged = sb_scatter_staged_smem(b.max_sb, kStageEntries);
+  const size_t smem_staged = sb_scatter_staged_smem(b.max_sb, b.max_sb_side, kStageEntries);
   if (smem_staged <= 100 * 1024) {
     if (smem_staged > 48 * 1024)
       TRY_CUDA(cudaFuncSetAttribute(k_sb_scatter_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -242,7 +243,7 @@ int choose_sb_log2(int tile_w, int tile_h) {
 }
 
 void fill_sb_layout(ViewBatch* b) {
-  uint32_t sb = 0, mx = 0;
+  uint32_t sb = 0, mx = 0, side = 1;
   for (int v = 0; v < b->num_views; ++v) {
     ViewDev& d = b->v[v];
     d.sb_base = sb;
@@ -250,9 +251,11 @@ void fill_sb_layout(ViewBatch* b) {
     const uint32_t c = uint32_t(sb_cols(d)) * uint32_t(sb_rows(d));
     sb += c;
     mx = c > mx ? c : mx;
+    side = std::max(side, uint32_t(std::max(sb_cols(d), sb_rows(d))));
   }
   b->num_sb = sb;
   b->max_sb = mx;
+  b->max_sb_side = side;
 }
 
 // ---------------------------------------------------------------------------

@@ -45,7 +45,7 @@ struct ViewBatch {
   uint32_t num_sb;     // sum of superblock counts
   uint32_t max_sb;     // largest per-view superblock count
   int32_t ppl;         // rasteriser pixels per lane (warp task = 32 * ppl pixels)
-  int32_t pad;
+  uint32_t max_sb_side;  // largest per-view superblock column or row count (<= 255)
   ViewDev v[DSPLAT_MAX_VIEWS];
 };
 

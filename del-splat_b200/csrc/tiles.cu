@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
                                                            const ViewBatch b,
                                                            const uint32_t* __restrict__ off, uint64_t capacity,
                                                            uint2* __restrict__ list1, uint32_t* __restrict__ flags) {
-  extern __shared__ uint32_t smem_ms[];  // [kMsWarps][nsb] counters, then [kMsWarps][256+256] masks
+  extern __shared__ uint32_t smem_ms[];  // [kMsWarps][nsb] counters, then [kMsWarps][2 * side] masks
   const uint32_t nchunk = npad / kMsChunk;
   const uint32_t v = blockIdx.x / nchunk, c = blockIdx.x % nchunk;
   const ViewDev& vd = b.v[v];
@@ -395,8 +395,9 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
   uint32_t* wc = smem_ms;
-  uint32_t* colmask = smem_ms + kMsWarps * b.max_sb + warp * 512;
-  uint32_t* rowmask = colmask + 256;
+  const uint32_t side = b.max_sb_side;
+  uint32_t* colmask = smem_ms + kMsWarps * b.max_sb + warp * 2 * side;
+  uint32_t* rowmask = colmask + side;
   for (int i = threadIdx.x; i < kMsWarps * nsb; i += kMsThreads) wc[i] = 0;
   __syncthreads();
   const size_t base = size_t(v) * npad + size_t(c) * kMsChunk + size_t(warp) * (kMsRounds * 32);
@@ -471,13 +472,15 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter(const uint32_t* __res
 // with more entries than the stage holds writes the same slots directly.
 // Shared memory (words): counters [8][max_sb], cursors [max_sb], stage
 // bases [max_sb + 2] (one spare word keeps the stage 8-byte aligned), masks
-// [8][512], then the stage (uint2[qcap]) and its superblock ids (u16[qcap]).
+// [8][2 * max_sb_side] (superblock columns, then rows), then the stage
+// (uint2[qcap]) and its superblock ids (u16[qcap]).
 // ---------------------------------------------------------------------------
 constexpr int kSubRounds = 2;
 constexpr int kSubRanks = kMsThreads * kSubRounds;  // 512 ranks per sub-pass
 
-size_t sb_scatter_staged_smem(uint32_t max_sb, uint32_t qcap) {
-  return (size_t(kMsWarps) * max_sb + 2 * size_t(max_sb) + 2 + kMsWarps * 512) * 4 + size_t(qcap) * 8 +
+size_t sb_scatter_staged_smem(uint32_t max_sb, uint32_t max_side, uint32_t qcap) {
+  return (size_t(kMsWarps) * max_sb + 2 * size_t(max_sb) + 2 + size_t(kMsWarps) * 2 * max_side) * 4 +
+         size_t(qcap) * 8 +
          ((size_t(qcap) + 1) / 2) * 4;
 }
 
@@ -500,9 +503,10 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_scatter_staged(const uint32_t
   uint32_t* wc = smem_ms;                     // [kMsWarps][nsb]
   uint32_t* cur = wc + kMsWarps * M;          // [nsb]
   uint32_t* sbase = cur + M;                  // [nsb + 1]
-  uint32_t* colmask = sbase + M + 2 + warp * 512;
-  uint32_t* rowmask = colmask + 256;
-  uint2* stage = reinterpret_cast<uint2*>(sbase + M + 2 + kMsWarps * 512);  // 10 M + 4098 words: 8-byte aligned
+  const uint32_t side = b.max_sb_side;
+  uint32_t* colmask = sbase + M + 2 + warp * 2 * side;
+  uint32_t* rowmask = colmask + side;
+  uint2* stage = reinterpret_cast<uint2*>(sbase + M + 2 + kMsWarps * 2 * side);  // 10 M + 2 + 16 side words: 8-byte aligned
   uint16_t* stage_sb = reinterpret_cast<uint16_t*>(stage + qcap);
   uint32_t* my = wc + warp * nsb;
   const uint32_t sb0 = vd.sb_base;
