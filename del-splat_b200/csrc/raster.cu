@@ -39,8 +39,8 @@
 // transmittance in front of each entry is rebuilt from the saved final value,
 // T_i = T_{i+1} / (1 - e_i), and the colour behind it is accumulated, so no
 // per-pixel list is stored.  Each lane sums its pixels' contributions in
-// registers as moments of w = dL/dq (sum w, sum w dy, sum w dy^2 -- dx is
-// fixed per lane), the warp reduces the nine per-entry sums with a
+// registers as moments of t = G dL/dalpha (sum t, sum t dy, sum t dy^2 --
+// dx is fixed per lane; w = dL/dq = -op/2 t is applied once per entry), the warp reduces the nine per-entry sums with a
 // transposed butterfly (9 + 5 shuffles instead of 45), and nine lanes add
 // the finished 2D gradient to the per-(view, point) record with one atomic
 // instruction.
@@ -538,8 +538,9 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
       for (int j = 0; j < k_staged; ++j) {
         const float4 ea = sm[j].a, eb = sm[j].b, ec = sm[j].c, ed = sm[j].d;
         const uint32_t pos = __float_as_uint(ed.z);
-        // v[]: this lane's sums over its pixels of (w dx, w dy, w dx^2,
-        // w dx dy, w dy^2, dL/dop, dL/dr, dL/dg) with w = dL/dq; gb = dL/db
+        // v[]: this lane's sums over its pixels of (t dx, t dy, t dx^2,
+        // t dx dy, t dy^2, t, dL/dr, dL/dg) with t = G dL/dalpha (its sum
+        // is dL/dop; w = dL/dq = -op/2 t); gb = dL/db
         float v[8], gb = 0.f;
 #pragma unroll
         for (int i = 0; i < 8; ++i) v[i] = 0.f;
@@ -547,8 +548,10 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
         const float dx = fx - ea.x;
         if (ec.y <= fx && fx <= ec.w) {
           const float kadxdx = ea.z * dx * dx, kb2dx = ea.w * dx;
-          const float mhop = -0.5f * eb.y;
-          float sw = 0.f, swdy = 0.f, swdyy = 0.f;
+          // moments of t = G dL/dalpha (v[5] = sum t, tdy = sum t dy, tdyy =
+          // sum t dy^2); w = dL/dq = -op/2 t, the factor is applied once per
+          // entry after the warp reduction
+          float tdy = 0.f, tdyy = 0.f;
 #pragma unroll
           for (int k = 0; k < PPL; ++k) {
             const float fy = float(iy0 + k * G::ROW_STEP) + 0.5f;
@@ -568,17 +571,15 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
             gb += wgt * d2[k];
             const float t = Gv * dLde;
             v[5] += t;
-            const float w = t * mhop;
-            const float wdy = w * dy;
-            sw += w;
-            swdy += wdy;
-            swdyy += wdy * dy;
+            const float tdy_p = t * dy;
+            tdy += tdy_p;
+            tdyy += tdy_p * dy;
           }
-          v[0] = sw * dx;
-          v[1] = swdy;
+          v[0] = v[5] * dx;
+          v[1] = tdy;
           v[2] = v[0] * dx;
-          v[3] = swdy * dx;
-          v[4] = swdyy;
+          v[3] = tdy * dx;
+          v[4] = tdyy;
         }
         if (__any_sync(0xffffffffu, any)) {
           // transposed butterfly: after the offset-16/8/4 steps lane L holds a
@@ -605,8 +606,9 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) gb += __shfl_xor_sync(0xffffffffu, gb, o);
           const float m0 = __shfl_sync(0xffffffffu, v[0], 0), m1 = __shfl_sync(0xffffffffu, v[0], 4);
-          // d px = -2 (A m0 + B m1), d py = -2 (B m0 + C m1), d A = m2,
-          // d B = 2 m3, d C = m4 (raw conic recovered from the staged one)
+          // with the w moments m_i = -op/2 (t moments): d px = -2 (A m0 +
+          // B m1), d py = -2 (B m0 + C m1), d A = m2, d B = 2 m3, d C = m4
+          // (raw conic recovered from the staged one)
           const float A = ea.z * kInvNegHalfLog2e, B = ea.w * (0.5f * kInvNegHalfLog2e),
                       C = eb.x * kInvNegHalfLog2e;
           const int k = lane >> 2;
@@ -614,6 +616,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
           if (k == 0) out = -2.f * (A * m0 + B * m1);
           if (k == 1) out = -2.f * (B * m0 + C * m1);
           if (k == 3) out = 2.f * v[0];
+          if (k < 5) out *= -0.5f * eb.y;  // the moments of t become moments of w = dL/dq
           float* dst = gv + 12 * size_t(__float_as_uint(ed.y));
           if ((lane & 3) == 0) atomicAdd(dst + k, out);
           if (lane == 1) atomicAdd(dst + 8, gb);
