@@ -11,8 +11,9 @@
 // per lane); with 16x16 or 32x32 tiles a slab of one tile (32 lanes x 2..8
 // pixels).  A lane's pixels share its column.  A warp stages 32 list entries
 // at a time into its own shared-memory slots (one coalesced index load + one
-// 48-byte record gather per lane), then every lane walks them with 128-bit
-// broadcast reads, amortising each read over its pixels.  The fused path
+// 48-byte record gather per lane; the next batch's index loads are issued
+// before the current batch is walked), then every lane walks them with
+// 128-bit broadcast reads, amortising each read over its pixels.  The fused path
 // reads the entries straight out of the superblock list (1-8 tiles per
 // side, see tiles.cu): a ballot over the 32 fetched entries keeps those whose
 // tile span meets the task's tiles, compacted in order, so no per-tile list
@@ -156,12 +157,17 @@ struct PackedSrc {
 // [pos0 - 32, pos0) (backwards) or [pos0, pos0 + 32) (forwards) into the
 // warp's slots, in walk order, each with its list position (set_pos);
 // return how many were staged.
+// load() reads a lane's list word ahead of time (a prefetch while the
+// previous batch is walked); stage() filters and gathers from it.
 struct TileWalk {  // a per-tile list (tile2idx / idx2pnt)
   const uint32_t* idx2pnt;
+  __device__ __forceinline__ uint2 load(uint32_t pos, bool valid) const {
+    return make_uint2(valid ? idx2pnt[pos] : 0u, 0u);
+  }
   template <class Src, class E>
-  __device__ __forceinline__ int stage(const Src& src, E* sm, uint32_t pos, bool valid, int lane) const {
+  __device__ __forceinline__ int stage(const Src& src, E* sm, uint2 en, uint32_t pos, bool valid, int lane) const {
     if (valid) {
-      src.stage(&sm[lane], idx2pnt[pos]);
+      src.stage(&sm[lane], en.x);
       sm[lane].set_pos(pos);
     }
     return __popc(__ballot_sync(0xffffffffu, valid));
@@ -174,12 +180,14 @@ struct TileWalk {  // a per-tile list (tile2idx / idx2pnt)
 struct SbWalkSpan {
   const uint2* list1;
   uint32_t lx, ly, nx;
+  __device__ __forceinline__ uint2 load(uint32_t pos, bool valid) const {
+    return valid ? list1[pos] : make_uint2(0u, 0u);
+  }
   template <class Src, class E>
-  __device__ __forceinline__ int stage(const Src& src, E* sm, uint32_t pos, bool valid, int lane) const {
+  __device__ __forceinline__ int stage(const Src& src, E* sm, uint2 en, uint32_t pos, bool valid, int lane) const {
     bool m = false;
     uint32_t g = 0;
     if (valid) {
-      const uint2 en = list1[pos];
       g = en.x;
       const uint32_t lr = en.y;
       m = lx < ((lr >> 8) & 15u) && lx + nx > (lr & 15u) && ly >= ((lr >> 4) & 15u) && ly < (lr >> 12);
@@ -257,9 +265,14 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
   const float fy_first = float(py0) + 0.5f, fy_last = float(py0 + G::SLAB_ROWS - 1) + 0.5f;
   const uint32_t inside = live;
   uint32_t hi = e;
+  uint2 en = hi > s ? walk.load(hi - 1u - uint32_t(lane), uint32_t(lane) < hi - s) : make_uint2(0u, 0u);
   while (hi > s) {
     const int cnt = int(min(32u, hi - s));
-    const int k_staged = walk.stage(src, sm, hi - 1u - uint32_t(lane), lane < cnt, lane);
+    const int k_staged = walk.stage(src, sm, en, hi - 1u - uint32_t(lane), lane < cnt, lane);
+    {  // the next batch's list words arrive while this batch is blended
+      const uint32_t hn = hi - uint32_t(cnt);
+      if (hn > s) en = walk.load(hn - 1u - uint32_t(lane), uint32_t(lane) < hn - s);
+    }
     __syncwarp();
     if (live) {
       for (int j = 0; j < k_staged; ++j) {
@@ -531,9 +544,13 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_bwd(
     PackedSrc src{rec + 3 * size_t(ig.v) * n};
     SbWalkSpan walk{list1, ig.lx, ig.ly, nx};
     float* gv = reinterpret_cast<float*>(grad2d + 3 * size_t(ig.v) * n);
-    for (uint32_t lo = max(s, lo_min); lo < e; lo += 32) {
+    const uint32_t lo0 = max(s, lo_min);
+    uint2 en = lo0 < e ? walk.load(lo0 + uint32_t(lane), uint32_t(lane) < e - lo0) : make_uint2(0u, 0u);
+    for (uint32_t lo = lo0; lo < e; lo += 32) {
       const int cnt = int(min(32u, e - lo));
-      const int k_staged = walk.stage(src, sm, lo + uint32_t(lane), lane < cnt, lane);
+      const int k_staged = walk.stage(src, sm, en, lo + uint32_t(lane), lane < cnt, lane);
+      // the next batch's list words arrive while this batch is processed
+      if (lo + 32u < e) en = walk.load(lo + 32u + uint32_t(lane), uint32_t(lane) < e - (lo + 32u));
       __syncwarp();
       for (int j = 0; j < k_staged; ++j) {
         const float4 ea = sm[j].a, eb = sm[j].b, ec = sm[j].c, ed = sm[j].d;
