@@ -164,6 +164,28 @@ def profiled_traffic(kernel_stage: str, views: int):
     return None
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (Linux /proc/cpuinfo), for the CPU baseline."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def single_thread_sample(scene, nthreads: int, tile_size: int):
+    """1-thread vs all-thread time of the workload's smallest view (the
+    reference's CPU path is single-threaded); returns (s 1 thread, s all
+    threads, view description)."""
+    i = min(range(len(scene.cameras)), key=lambda k: scene.cameras[k].width * scene.cameras[k].height)
+    t1, cam = cpu_sample(scene, i, 1, tile_size)
+    tn, _ = cpu_sample(scene, i, nthreads, tile_size)
+    return t1, tn, f"{cam.width}x{cam.height}"
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -379,7 +401,7 @@ def run_zbuffer(args, rank, world, local):
         t2i, i2p, _ = oracle.tile2pnt(xyd_h, aabb, W, H, ts)
         oracle.circle_splat_tiled(W, H, ts, t2i, i2p, xyd_h, sc.radius_px)
         cpu_s = time.perf_counter() - t0
-        cpu = {"value": 1.0 / cpu_s, "unit": "frames/s", "cores": 1, "kind": "port",
+        cpu = {"value": 1.0 / cpu_s, "unit": "frames/s", "cores": 1, "kind": "port", "cpu_model": cpu_model(),
                "sample": "one full frame: tile lists + tiled circle painter (oracle C++ restatement of "
                          "del-splat-cpu's sorted painter), 1 thread; projection excluded"}
     peak, peak_kind = peaks()
@@ -702,7 +724,12 @@ def main():
         try:
             nth = os.cpu_count() or 1
             rate, desc = cpu_workload_rate(base, nth, 16)  # the reference's tile size; results do not depend on it
-            cpu = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port", "sample": desc}
+            t1, tn, res = single_thread_sample(base, nth, 16)
+            cpu = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port", "sample": desc,
+                   "cpu_model": cpu_model(),
+                   "single_thread": {"view": res, "s_per_view_1_thread": t1, "s_per_view_all_threads": tn,
+                                     "estimated_value_1_thread": rate * tn / t1,
+                                     "note": "workload rate scaled by this view's all-thread / 1-thread time"}}
         except Exception as ex:  # the CPU baseline must not hide the GPU result
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
 
