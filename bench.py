@@ -514,15 +514,15 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
+    if args.impl == "reference":  # CPU only: no process group, no GPU
+        run_reference(args, int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")))
+        return
     rank, world, local = dist_setup()
-    if args.impl == "reference":
-        run_reference(args, rank, world)
-        return
-    if args.workload == "zbuffer":
-        run_zbuffer(args, rank, world, local)
-        return
-    if args.workload == "train4m":
-        run_train4m(args, rank, world, local)
+    if args.workload in ("zbuffer", "train4m"):
+        (run_zbuffer if args.workload == "zbuffer" else run_train4m)(args, rank, world, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
 
     from dsplat import _native, scenes
@@ -772,7 +772,7 @@ def main():
                                   "per-tile-list design would read them, while this kernel reads point records "
                                   "through L2 and shared memory: traffic (DRAM bytes per launch, ncu, scaled "
                                   "by views from the committed profile) shows the rasterisers are not HBM-bound "
-                                  "but instruction-issue bound (85-87% issue slots busy)")},
+                                  "but instruction-issue bound (79% of issue slots busy, top stall not-selected)")},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_vps, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4},
             "gpu_launches": int(launches),
