@@ -180,3 +180,18 @@ def test_large_splats_take_the_direct_scatter_path(orc, dev):
     assert needed > len(sc.cameras) * 6 * 3072
     for v in range(len(sc.cameras)):
         _check_view(orc, batch, sc, v, 8)
+
+
+def test_thousands_of_superblocks_take_the_unstaged_scatter(orc, dev):
+    """A 3072x3072 view at 8x8 tiles has 48x48 = 2304 superblocks: the staged
+    superblock scatter would need more than its 100 KB shared-memory budget,
+    so the lists are built by the unstaged kernel.  Lists, images and stops
+    stay bit-exact."""
+    sc = scenes.config0(seed=23, n=4000, size=(64, 64))
+    sc.cameras = [scenes.Camera.look_at_origin((0.1, 0.3, -3.0), 3072, 3072)]
+    p = params_of(sc, dev)
+    batch = GaussBatch(sc.n, sc.cameras, 8, sc.sh_degree, pair_capacity=1 << 20, device=dev, pixels_per_lane=2)
+    assert int(batch.layout.sb_log2[0]) == 3 and int(batch.layout.num_sb) == 48 * 48
+    batch.ensure_capacity(p)
+    assert batch.status()[0] == 0
+    _check_view(orc, batch, sc, 0, 8)
