@@ -61,7 +61,8 @@ __global__ void k_order_hist(const ViewBatch, const uint32_t*, uint32_t, const u
 __global__ void k_order_scan(uint32_t*);
 __global__ void k_order_scatter(const ViewBatch, const uint32_t*, uint32_t, const uint32_t*, uint32_t*, uint32_t*);
 cudaError_t raster_fwd_aos(cudaStream_t, int, int, int, float*, const float*, const float*, const float*, const float*,
-                           const float*, const uint32_t*, const uint32_t*, float*, uint32_t*);
+                           const float*, const uint32_t*, const uint32_t*, float*, uint32_t*, bool);
+cudaError_t expf_cr_launch(cudaStream_t, size_t, const float*, float*);
 cudaError_t circle_splat_tiles(cudaStream_t, int, int, int, float*, const float*, const float*, const float*,
                                const uint32_t*, const uint32_t*);
 
@@ -560,18 +561,37 @@ int dsplat_gauss_tile2idx_idx2pnt(dsplat_stream stream, uint32_t num_pnt, const 
                     workspace_bytes);
 }
 
+int dsplat_gauss_rasterize_pnt2splat2_stop(dsplat_stream stream, uint32_t img_w, uint32_t img_h, float* pix2rgb,
+                                           const float* pnt2pixxydepth, const float* pnt2pixconvinv,
+                                           const float* pnt2pixaabb, const float* pnt2opacity, const float* pnt2rgb,
+                                           uint32_t tile_size, const uint32_t* tile2idx, const uint32_t* idx2pnt,
+                                           float* pix2transmit, uint32_t* pix2stop, int32_t stop_rule) {
+  if (!ts_ok(tile_size)) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
+  if (stop_rule != DSPLAT_STOP_CPU && stop_rule != DSPLAT_STOP_CUDA)
+    return fail(DSPLAT_ERR_INVALID_ARG, "stop_rule must be DSPLAT_STOP_CPU or DSPLAT_STOP_CUDA");
+  if (img_w == 0 || img_h == 0) return DSPLAT_OK;
+  if (!pix2rgb || !tile2idx) return fail(DSPLAT_ERR_INVALID_ARG, "null pointer");
+  TRY_CUDA(raster_fwd_aos(static_cast<cudaStream_t>(stream), int(tile_size), int(img_w), int(img_h), pix2rgb,
+                          pnt2pixxydepth, pnt2pixconvinv, pnt2pixaabb, pnt2opacity, pnt2rgb, tile2idx, idx2pnt,
+                          pix2transmit, pix2stop, stop_rule == DSPLAT_STOP_CUDA),
+           "raster_fwd_aos");
+  return DSPLAT_OK;
+}
+
 int dsplat_gauss_rasterize_pnt2splat2(dsplat_stream stream, uint32_t img_w, uint32_t img_h, float* pix2rgb,
                                       const float* pnt2pixxydepth, const float* pnt2pixconvinv,
                                       const float* pnt2pixaabb, const float* pnt2opacity, const float* pnt2rgb,
                                       uint32_t tile_size, const uint32_t* tile2idx, const uint32_t* idx2pnt,
                                       float* pix2transmit, uint32_t* pix2stop) {
-  if (!ts_ok(tile_size)) return fail(DSPLAT_ERR_UNSUPPORTED, "tile_size must be 8, 16 or 32");
-  if (img_w == 0 || img_h == 0) return DSPLAT_OK;
-  if (!pix2rgb || !tile2idx) return fail(DSPLAT_ERR_INVALID_ARG, "null pointer");
-  TRY_CUDA(raster_fwd_aos(static_cast<cudaStream_t>(stream), int(tile_size), int(img_w), int(img_h), pix2rgb,
-                          pnt2pixxydepth, pnt2pixconvinv, pnt2pixaabb, pnt2opacity, pnt2rgb, tile2idx, idx2pnt,
-                          pix2transmit, pix2stop),
-           "raster_fwd_aos");
+  return dsplat_gauss_rasterize_pnt2splat2_stop(stream, img_w, img_h, pix2rgb, pnt2pixxydepth, pnt2pixconvinv,
+                                                pnt2pixaabb, pnt2opacity, pnt2rgb, tile_size, tile2idx, idx2pnt,
+                                                pix2transmit, pix2stop, DSPLAT_STOP_CPU);
+}
+
+int dsplat_expf_cr(dsplat_stream stream, uint64_t n, const float* x, float* y) {
+  if (n == 0) return DSPLAT_OK;
+  if (!x || !y) return fail(DSPLAT_ERR_INVALID_ARG, "null pointer");
+  TRY_CUDA(expf_cr_launch(static_cast<cudaStream_t>(stream), size_t(n), x, y), "k_expf_cr");
   return DSPLAT_OK;
 }
 
@@ -647,8 +667,10 @@ int dsplat_point_rasterize_pix_zbuffer(dsplat_stream stream, uint32_t num_pnt, c
     return fail(DSPLAT_ERR_INVALID_ARG, "null pointer");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   k_fill_u64<<<blocks_for(npix, 256), 256, 0, st>>>(zbuf, npix, ~0ull); count_launch();
-  if (num_pnt > 0)
-    k_point_zbuf<<<blocks_for(num_pnt, 256), 256, 0, st>>>(num_pnt, pnt2pixxyndcz, int(img_w), int(img_h), zbuf); count_launch();
+  if (num_pnt > 0) {
+    k_point_zbuf<<<blocks_for(num_pnt, 256), 256, 0, st>>>(num_pnt, pnt2pixxyndcz, int(img_w), int(img_h), zbuf);
+    count_launch();
+  }
   k_point_resolve<<<blocks_for(npix, 256), 256, 0, st>>>(npix, zbuf, pnt2pixxyndcz, pnt2rgb, pix2rgb, pix2unitdepth,
                                                          pix2winner); count_launch();
   TRY_CUDA(cudaGetLastError(), "point zbuffer");

@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include "dsplat.h"
+#include "exp_tables.cuh"
 
 #include <atomic>
 
@@ -102,70 +103,9 @@ __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); 
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
 
-// Deterministic exp(x): Cody-Waite reduction x = n*ln2 + r with ln2 split in
-// a high part that has 9 trailing zero bits (so n*LN2_HI is exact for
-// |n| < 512) and a low part, then the degree-7 Taylor polynomial of e^r on
-// |r| <= ln2/2 (truncation error < 6e-9 relative) and an exact 2^n scaling.
-// Only IEEE-exact operations are used, so the CPU oracle reproduces every
-// bit.  Results below 2^-126 flush to zero.
-__device__ __forceinline__ float dexp(float x) {
-  if (x != x) return x;
-  if (x < -87.0f) return 0.0f;
-  if (x > 88.5f) return __int_as_float(0x7f800000);
-  const float n = rintf(fm(x, 1.44269502162933349609375f));
-  float r = fs(x, fm(n, 0.693145751953125f));
-  r = fs(r, fm(n, 1.428606765330187045e-06f));
-  float p = 1.984126984126984e-04f;  // 1/5040
-  p = fa(fm(p, r), 1.388888888888889e-03f);  // 1/720
-  p = fa(fm(p, r), 8.333333333333333e-03f);  // 1/120
-  p = fa(fm(p, r), 4.166666666666667e-02f);  // 1/24
-  p = fa(fm(p, r), 1.666666666666667e-01f);  // 1/6
-  p = fa(fm(p, r), 0.5f);
-  p = fa(fm(p, r), 1.0f);
-  p = fa(fm(p, r), 1.0f);
-  const int ni = (int)n;
-  if (ni < -126) return 0.0f;
-  return fm(p, __int_as_float((ni + 127) << 23));
-}
-
 // Fused multiply-add with a single rounding (IEEE fma; the CPU oracle's
 // std::fma gives the same bits).
 __device__ __forceinline__ float ff(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-
-// The rasterisers evaluate exp(-q/2) as 2^y with y = q * (-log2(e)/2); the
-// factor is folded into the staged conic, so y comes out of the quadratic
-// form directly.
-constexpr float kNegHalfLog2e = -0.72134752044448170368f;
-constexpr float kInvNegHalfLog2e = -1.38629436111989061883f;  // -2 ln 2
-
-// Deterministic 2^y: y = n + f with n = nearest integer (the 1.5 * 2^23
-// addition rounds y in the binade where the float spacing is 1; n is read
-// back from the sum's bits), |f| <= 1/2, then a degree-5 polynomial
-// 1 + f (c1 + f (c2 + ...)) fitted to 2^f on [-1/2, 1/2] by minimising the
-// largest relative error (linear program on a dense grid, oracle/fit_exp2.py;
-// 6.8e-8 before rounding, 2.2e-7 measured over every float f of the
-// interval after float rounding and evaluation) in Horner form with fused
-// multiply-adds, and the exact scaling by 2^n through the exponent field.  Every step is an exactly rounded IEEE operation, so the CPU oracle
-// reproduces the result bit for bit.  Outside (-125, 123): 0 below, +inf
-// above, NaN stays NaN.
-constexpr float kExp2C1 = 0.6931465864181519f, kExp2C2 = 0.24022166430950165f, kExp2C3 = 0.055510472506284714f,
-                kExp2C4 = 0.009674952365458012f, kExp2C5 = 0.0013202981790527701f;
-__device__ __forceinline__ float exp2_det(float y) {
-  if (!(fabsf(__fadd_rn(y, 1.f)) < 124.f)) {
-    if (y != y) return y;
-    return y < 0.f ? 0.f : __int_as_float(0x7f800000);
-  }
-  const float t = __fadd_rn(y, 12582912.f);
-  const float f = __fsub_rn(y, __fsub_rn(t, 12582912.f));
-  float p = kExp2C5;
-  p = ff(p, f, kExp2C4);
-  p = ff(p, f, kExp2C3);
-  p = ff(p, f, kExp2C2);
-  p = ff(p, f, kExp2C1);
-  p = ff(p, f, 1.f);
-  const uint32_t n = uint32_t(__float_as_int(t) - __float_as_int(12582912.f));
-  return __int_as_float(int(uint32_t(__float_as_int(p)) + (n << 23)));
-}
 
 // Packed two-wide FP32 (sm_100 f32x2): each element is the exactly rounded
 // IEEE result of the scalar operation, so packed and scalar sequences give
@@ -208,32 +148,127 @@ __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
   return r;
 }
 
-// exp2_det2_inrange: exp2_det's fast path on both elements, packed; equal
-// to exp2_det for elements in (-125, 123).  A caller that has bounded y to
-// that range (see fwd_slab) uses it directly.
-__device__ __forceinline__ f2 exp2_det2_inrange(f2 y) {
-  const f2 magic = f2_dup(12582912.f);
-  const f2 t = add2(y, magic);
-  const f2 f = sub2(y, sub2(t, magic));
-  f2 p = f2_dup(kExp2C5);
-  p = fma2(p, f, f2_dup(kExp2C4));
-  p = fma2(p, f, f2_dup(kExp2C3));
-  p = fma2(p, f, f2_dup(kExp2C2));
-  p = fma2(p, f, f2_dup(kExp2C1));
-  p = fma2(p, f, f2_dup(1.f));
-  // n << 23 = (bits(t) - bits(1.5 * 2^23)) << 23 = bits(t) << 23 modulo 2^32
-  // (the low 9 bits of bits(1.5 * 2^23) are zero): one shift-add per element
-  return f2_make(__uint_as_float(__float_as_uint(f2_lo(p)) + (__float_as_uint(f2_lo(t)) << 23)),
-                 __uint_as_float(__float_as_uint(f2_hi(p)) + (__float_as_uint(f2_hi(t)) << 23)));
+__device__ __forceinline__ f2 neg2(f2 a) { return a ^ 0x8000000080000000ull; }
+
+// ---------------------------------------------------------------------------
+// expf_cr: e^x correctly rounded to single precision (the float nearest to
+// the exact value), for every float x.  The blend evaluates exp(-q/2) with
+// it, so its values are those of del-splat-cpu's f32 `exp` wherever that is
+// correctly rounded too (glibc 2.39's expf is, except on about 1 input in
+// 11,500 of [-110, 0], where it is one unit in the last place off).
+//
+// Fast path, |x| <= 87, single precision only:
+//   k = nearest integer to x * 64/ln2 (the 1.5 * 2^23 addition rounds it);
+//   r = x - k ln2/64 with ln2/64 = C1 + C2 + C3: k C1 and k C2 are exact
+//     (11-bit constants, |k| < 2^13) and so are both subtractions, which
+//     leaves rh exact and rl = -k C3 (|rl| < 2^-22) as a correction;
+//   e^r - 1 = rh + rl (1 + rh) + rh^2 (1/2 + rh/6 + rh^2/24) + O(2^-44);
+//   2^(j/64) (j = k mod 64) as the float pair TH + TL from a 64-entry table;
+//   y = (TH + TL) e^r summed as s + ylo with an exact product TH rh and a
+//     Fast2Sum, then rounded.  If ylo +- 2^-37 round to the same float the
+//     exact value rounds to it too (rounding is monotonic and the error of
+//     s + ylo is below 2^-37 for y in [0.99, 2)), so that float is the
+//     correctly rounded result; it is scaled by 2^(k div 64) exactly.
+// Otherwise (|x| > 87, NaN, or the rounding test failed -- about 4e-5 of
+// the inputs), expf_cr_slow evaluates the same reduction in double precision
+// (degree-6 polynomial, 2^(j/64) rounded to double) and rounds the double
+// once to float, which also produces subnormal results, 0 and infinity.
+// Both paths were compared with the correctly rounded value (float)e^x for
+// all 2^32 float inputs and agree everywhere; every operation is an exactly
+// rounded IEEE operation, so the result does not depend on the compiler.
+// ---------------------------------------------------------------------------
+constexpr float kExpMagic = 12582912.f;                            // 1.5 * 2^23
+constexpr float kExpP3 = 0x1.555556p-3f, kExpP4 = 0x1.555556p-5f;  // 1/6, 1/24
+constexpr float kExpTie = 0x1p-37f;
+constexpr float kExpFastMax = 87.f;
+
+static __device__ __noinline__ float expf_cr_slow(float x) {
+  if (x != x) return x;
+  if (x > 89.f) return __int_as_float(0x7f800000);
+  if (x < -104.f) return 0.f;
+  const double xd = double(x);
+  const double t = __fma_rn(xd, kExpK64d, 0x1.8p52);
+  const double kd = __dsub_rn(t, 0x1.8p52);
+  double r = __fma_rn(kd, -kExpL1d, xd);
+  r = __fma_rn(kd, -kExpL2d, r);
+  const int k = __double2loint(t);  // the low word of t holds k
+  double p = 1.0 / 720;
+  p = __fma_rn(p, r, 1.0 / 120);
+  p = __fma_rn(p, r, 1.0 / 24);
+  p = __fma_rn(p, r, 1.0 / 6);
+  p = __fma_rn(p, r, 0.5);
+  p = __fma_rn(p, r, 1.0);
+  const double tj = __ldg(&g_exp2_64d[k & 63]);
+  double y = __fma_rn(tj, __dmul_rn(p, r), tj);
+  y = __dmul_rn(y, __hiloint2double(((k >> 6) + 1023) << 20, 0));
+  return __double2float_rn(y);
 }
-// exp2_det on both elements: the fast path runs packed, the (rare) case of
-// an element outside (-125, 123) falls back to the scalar function; every
-// element equals exp2_det of it.
-__device__ __forceinline__ f2 exp2_det2(f2 y) {
-  const float y0 = f2_lo(y), y1 = f2_hi(y);
-  const f2 yp1 = add2(y, f2_dup(1.f));
-  if (!(fabsf(f2_lo(yp1)) < 124.f) || !(fabsf(f2_hi(yp1)) < 124.f)) return f2_make(exp2_det(y0), exp2_det(y1));
-  return exp2_det2_inrange(y);
+
+// The fast path on one element with its table entry T = 2^(j/64)
+// (j = expf_cr_j(x)); *ok is false when the result must come from
+// expf_cr_slow.
+__device__ __forceinline__ uint32_t expf_cr_j(float x) {
+  return __float_as_uint(__fmaf_rn(x, kExpK64, kExpMagic)) & 63u;
+}
+__device__ __forceinline__ float expf_cr_fast(float x, float2 T, bool* ok) {
+  const float tk = __fmaf_rn(x, kExpK64, kExpMagic);
+  const float kf = __fsub_rn(tk, kExpMagic);
+  const float r1 = __fmaf_rn(kf, -kExpC1, x);
+  const float rh = __fmaf_rn(kf, -kExpC2, r1);
+  const float rl = __fmul_rn(kf, -kExpC3);
+  const float w = __fmaf_rn(rl, rh, rl);
+  const float r2 = __fmul_rn(rh, rh);
+  float p = __fmaf_rn(rh, kExpP4, kExpP3);
+  p = __fmaf_rn(p, rh, 0.5f);
+  const float tail = __fmaf_rn(r2, p, w);
+  const float ph = __fmul_rn(T.x, rh), pl = __fmaf_rn(T.x, rh, -ph);
+  const float s = __fadd_rn(T.x, ph), e1 = __fsub_rn(ph, __fsub_rn(s, T.x));
+  const float a = __fadd_rn(__fmaf_rn(T.x, tail, pl), e1);
+  const float ylo = __fadd_rn(a, __fmaf_rn(T.y, rh, T.y));
+  const float ra = __fadd_rn(s, __fadd_rn(ylo, kExpTie)), rb = __fadd_rn(s, __fsub_rn(ylo, kExpTie));
+  *ok = ra == rb && fabsf(x) <= kExpFastMax;
+  return __uint_as_float(__float_as_uint(ra) + ((__float_as_uint(tk) << 17) & 0xff800000u));
+}
+
+// Scalar form, table read from global memory.
+__device__ __forceinline__ float expf_cr(float x) {
+  bool ok;
+  const float y = expf_cr_fast(x, __ldg(&g_exp2_64[expf_cr_j(x)]), &ok);
+  return ok ? y : expf_cr_slow(x);
+}
+
+// Packed form for two elements, table in shared memory (tab: a copy of
+// g_exp2_64).  RANGE: check |x| <= 87 per element (a caller that has bounded
+// x for a whole batch passes false).  Each element equals expf_cr of it.
+template <bool RANGE>
+__device__ __forceinline__ f2 expf_cr2(f2 x, const float2* tab) {
+  const f2 tk = fma2(x, f2_dup(kExpK64), f2_dup(kExpMagic));
+  const f2 kf = sub2(tk, f2_dup(kExpMagic));
+  const f2 r1 = fma2(kf, f2_dup(-kExpC1), x);
+  const f2 rh = fma2(kf, f2_dup(-kExpC2), r1);
+  const f2 rl = mul2(kf, f2_dup(-kExpC3));
+  const f2 w = fma2(rl, rh, rl);
+  const f2 r2 = mul2(rh, rh);
+  f2 p = fma2(rh, f2_dup(kExpP4), f2_dup(kExpP3));
+  p = fma2(p, rh, f2_dup(0.5f));
+  const f2 tail = fma2(r2, p, w);
+  const uint32_t b0 = __float_as_uint(f2_lo(tk)), b1 = __float_as_uint(f2_hi(tk));
+  const float2 t0 = tab[b0 & 63u], t1 = tab[b1 & 63u];
+  const f2 th = f2_make(t0.x, t1.x), tl = f2_make(t0.y, t1.y);
+  const f2 ph = mul2(th, rh), pl = fma2(th, rh, neg2(ph));
+  const f2 s = add2(th, ph), e1 = sub2(ph, sub2(s, th));
+  const f2 a = add2(fma2(th, tail, pl), e1);
+  const f2 ylo = add2(a, fma2(tl, rh, tl));
+  const f2 ra = add2(s, add2(ylo, f2_dup(kExpTie))), rb = add2(s, sub2(ylo, f2_dup(kExpTie)));
+  float y0 = __uint_as_float(__float_as_uint(f2_lo(ra)) + ((b0 << 17) & 0xff800000u));
+  float y1 = __uint_as_float(__float_as_uint(f2_hi(ra)) + ((b1 << 17) & 0xff800000u));
+  bool ok = ra == rb;
+  if (RANGE) ok = ok && fabsf(f2_lo(x)) <= kExpFastMax && fabsf(f2_hi(x)) <= kExpFastMax;
+  if (!ok) {  // rare: settle each element on its own
+    if (!(f2_lo(ra) == f2_lo(rb) && fabsf(f2_lo(x)) <= kExpFastMax)) y0 = expf_cr_slow(f2_lo(x));
+    if (!(f2_hi(ra) == f2_hi(rb) && fabsf(f2_hi(x)) <= kExpFastMax)) y1 = expf_cr_slow(f2_hi(x));
+  }
+  return f2_make(y0, y1);
 }
 
 // Hardware approximations (PTX ex2.approx / rcp.approx, flush-to-zero) for
@@ -249,9 +284,12 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return r;
 }
 
-// splat_gauss.cu:105 `alpha_sum > 0.999` is a double comparison; for a float
-// alpha_sum it is exactly `alpha_sum >= 0.999f`.
-constexpr float kAlphaBreak = 0.999f;
+// Early exit of the front-to-back blend: del-splat-cpu stops once the f32
+// alpha sum exceeds 0.999f (pnt2pixxyndcz.rs:93, `alpha_sum > 0.999` with an
+// f32 left side).  The reference's CUDA kernel compares in double
+// (splat_gauss.cu:105), which for a float sum is `>= 0.999f`; the two rules
+// differ only when the sum equals 0.999f exactly.
+constexpr float kAlphaStop = 0.999f;
 
 // tile_acceleration.h:43-46
 __device__ __forceinline__ uint32_t depth_bits(float ndcz) {

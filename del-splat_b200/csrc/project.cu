@@ -308,8 +308,8 @@ __global__ void __launch_bounds__(kProjThreads) k_fused_project(
   const uint32_t g = g0 + threadIdx.x;
   if (g >= n) return;
   const float p[3] = {means[3 * g], means[3 * g + 1], means[3 * g + 2]};
-  const float s[3] = {dexp(log_scales[3 * g]), dexp(log_scales[3 * g + 1]),
-                      dexp(log_scales[3 * g + 2])};
+  const float s[3] = {expf_cr(log_scales[3 * g]), expf_cr(log_scales[3 * g + 1]),
+                      expf_cr(log_scales[3 * g + 2])};
   const float q[4] = {quats[4 * g], quats[4 * g + 1], quats[4 * g + 2], quats[4 * g + 3]};
   const float nrm = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
   const float qn[4] = {q[0] / nrm, q[1] / nrm, q[2] / nrm, q[3] / nrm};

@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(128) k_project_bwd_geom(uint32_t n, const floa
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n) return;
   const float p[3] = {means[3 * g], means[3 * g + 1], means[3 * g + 2]};
-  const float s[3] = {dexp(log_scales[3 * g]), dexp(log_scales[3 * g + 1]), dexp(log_scales[3 * g + 2])};
+  const float s[3] = {expf_cr(log_scales[3 * g]), expf_cr(log_scales[3 * g + 1]), expf_cr(log_scales[3 * g + 2])};
   const float dd[3] = {s[0] * s[0], s[1] * s[1], s[2] * s[2]};
   const float q[4] = {quats[4 * g], quats[4 * g + 1], quats[4 * g + 2], quats[4 * g + 3]};
   const float nrm = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);

@@ -4,7 +4,7 @@
 // from the end (nearest: largest ndc_z) to the start; skip entries whose
 // 3-sigma box does not contain the pixel centre (ix+.5, iy+.5);
 // e = exp(-q/2) * opacity with q = d^T conic d; rgb += c*T*e; T *= 1-e;
-// alpha_sum += T*e; stop once alpha_sum > 0.999.
+// alpha_sum += T*e; stop once alpha_sum > 0.999f.
 //
 // B200 structure: the unit of work is a warp task.  With 8x8 tiles a task
 // covers two horizontally adjacent tiles of one superblock (16x8 pixels, 4
@@ -19,7 +19,7 @@
 // tile span meets the task's tiles, compacted in order, so no per-tile list
 // is ever materialised.  The forward evaluates a lane's pixels in pairs with
 // packed f32x2 arithmetic; an entry whose exponent is bounded over its whole
-// box at staging skips exp2_det's range check, and one whose box holds every
+// box at staging skips expf_cr's range check, and one whose box holds every
 // row of the slab skips the per-slot row test (the same bits, fewer
 // instructions; the backward measured slower with the row hoist).  A forward
 // warp stops fetching as soon as all its pixels terminated (__any_sync), so
@@ -27,13 +27,15 @@
 // Warps pull tasks from a global counter (work stealing), longest first: one
 // persistent launch covers views of different resolutions.
 //
-// The blend arithmetic is a fixed sequence of exactly rounded IEEE
-// operations (multiply, add, fused multiply-add) with exp(-q/2) evaluated by
-// exp2_det(); the oracle performs the same sequence, so images, final
-// transmittances and every early-exit decision agree bit for bit.  Versus the
-// reference's expression order the per-pixel values differ only in rounding:
-// y = k q is evaluated as (kA dx) dx + (k2B dx + kC dy) dy, colours
-// accumulate with fma, and T <- T - T alpha replaces T <- T (1 - alpha).
+// The blend arithmetic is del-splat-cpu's (pnt2pixxyndcz.rs:86-93),
+// operation for operation in single precision with no fused multiply-adds:
+// q = A dx dx + B (dx dy + dy dx) + C dy dy, e = exp(-q/2) opacity with the
+// correctly rounded expf_cr, e_out = T e, rgb += c e_out per channel,
+// T *= 1 - e, alpha_sum += e_out, stop once alpha_sum > 0.999f.  The oracle
+// performs the same sequence with exp evaluated in double and rounded once
+// to float, so images, final transmittances and stop positions agree bit for
+// bit; against del-splat-cpu itself (glibc expf) they differ only where
+// glibc's expf is not correctly rounded.
 //
 // Backward (no reference counterpart): the same walk in reverse
 // (back-to-front) from the saved stop position up to the list end; the
@@ -55,6 +57,11 @@ constexpr int kRasterWarps = 4;  // warps per CTA (independent tasks)
 constexpr int kFwdGroup8 = 2;    // 8x8 tiles per forward task
 constexpr int kBwdGroup8 = 2;    // 8x8 tiles per backward task (4 measured slower: registers, partial overlaps)
 
+// The backward evaluates exp(-q/2) as 2^(k q) with k = -log2(e)/2 folded
+// into the staged conic (hardware ex2.approx; see k_raster_bwd).
+constexpr float kNegHalfLog2e = -0.72134752044448170368f;
+constexpr float kInvNegHalfLog2e = -1.38629436111989061883f;  // -2 ln 2
+
 struct Ent {  // one staged list entry (64 bytes), backward
   float4 a;   // px, py, k A, k 2B   (k = -log2(e)/2: exp(-q/2) = 2^(k q))
   float4 b;   // k C, opacity, r, g
@@ -65,33 +72,35 @@ struct Ent {  // one staged list entry (64 bytes), backward
 
 // A staged entry for the forward, whose pixel slots are evaluated in pairs
 // with packed two-wide FP32: every value a pair uses is stored twice, so a
-// 64-bit shared load yields the packed operand (96 bytes).
+// 64-bit shared load yields the packed operand (96 bytes).  The conic is
+// kept as the reference reads it: (A, B, C) = (m0, m1, m2) with 2 m1 staged
+// (exact), px and m0 once (they enter through the per-lane column term).
 struct EntP {
-  float4 a;  // px, px, py, py
-  float4 b;  // k A, k A, k 2B, k 2B
-  float4 c;  // k C, k C, opacity, opacity
-  float4 d;  // r, r, g, g
-  float4 e;  // b, b, box x0, box x1
-  float4 f;  // box y0, box y1, exponent in range (0/1 bits), list position (bits)
-  __device__ __forceinline__ void set_pos(uint32_t pos) { f.w = __uint_as_float(pos); }
+  float4 a;  // py, py, 2B, 2B
+  float4 b;  // C, C, opacity, opacity
+  float4 c;  // r, r, g, g
+  float4 d;  // b, b, px, A
+  float4 e;  // box x0, box x1, box y0, box y1
+  float4 f;  // exponent in expf_cr's fast range (0/1 bits), list position (bits), -, -
+  __device__ __forceinline__ void set_pos(uint32_t pos) { f.y = __uint_as_float(pos); }
 };
 
 __device__ __forceinline__ void make_entp(EntP* dst, float px, float py, float A, float B, float C, float op, float r,
                                           float g, float b, float x0, float y0, float x1, float y1) {
-  const float kA = fm(A, kNegHalfLog2e), k2B = fm(fa(B, B), kNegHalfLog2e), kC = fm(C, kNegHalfLog2e);
-  // The exponent y = kA dx^2 + k2B dx dy + kC dy^2 of every pixel centre in
-  // the box is bounded in magnitude by the same sum of absolute terms at the
-  // box's farthest corner; below 100 (rounding adds far less than the margin
-  // to 123) exp2_det's range check can be skipped for this entry.  NaN or
-  // infinite terms fail the test.
+  // q = A dx^2 + 2B dx dy + C dy^2 of every pixel centre in the box is
+  // bounded in magnitude by the same sum of absolute terms at the box's
+  // farthest corner; below 170 (rounding adds far less than the margin to
+  // 174) every exponent -q/2 of the entry lies in expf_cr's fast range and
+  // the per-pixel range check is skipped.  NaN or infinite terms fail it.
+  const float B2 = fa(B, B);
   const float dxm = fmaxf(fabsf(x0 - px), fabsf(x1 - px)), dym = fmaxf(fabsf(y0 - py), fabsf(y1 - py));
-  const float mag = fabsf(kA) * dxm * dxm + fabsf(k2B) * dxm * dym + fabsf(kC) * dym * dym;
-  dst->a = make_float4(px, px, py, py);
-  dst->b = make_float4(kA, kA, k2B, k2B);
-  dst->c = make_float4(kC, kC, op, op);
-  dst->d = make_float4(r, r, g, g);
-  dst->e = make_float4(b, b, x0, x1);
-  dst->f = make_float4(y0, y1, __uint_as_float(mag < 100.f ? 1u : 0u), 0.f);
+  const float mag = fabsf(A) * dxm * dxm + fabsf(B2) * dxm * dym + fabsf(C) * dym * dym;
+  dst->a = make_float4(py, py, B2, B2);
+  dst->b = make_float4(C, C, op, op);
+  dst->c = make_float4(r, r, g, g);
+  dst->d = make_float4(b, b, px, A);
+  dst->e = make_float4(x0, x1, y0, y1);
+  dst->f = make_float4(__uint_as_float(mag < 170.f ? 1u : 0u), 0.f, 0.f, 0.f);
 }
 
 // The staged conic, scaled so that y = k q = kA dx^2 + (k2B dx + kC dy) dy.
@@ -214,8 +223,11 @@ __device__ __forceinline__ float quad_y(float kC, float dy, float kb2dx, float k
 // (pixel done, row outside the entry's box) are uniform across the warp most
 // of the time.
 // ---------------------------------------------------------------------------
-template <int TS, int PPL_, class Walk, class Src>
-__device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, EntP* sm, uint32_t s, uint32_t e,
+// CUDA_STOP: the stop test of the reference's CUDA kernel (alpha_sum >=
+// 0.999f, its double comparison) instead of del-splat-cpu's (> 0.999f).
+template <int TS, int PPL_, bool CUDA_STOP, class Walk, class Src>
+__device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, EntP* sm, const float2* tab, uint32_t s,
+                                         uint32_t e,
                                          int px0, int py0, int w, int h, int xend, bool accumulate,
                                          float* __restrict__ out_rgb, size_t pix_base, float* __restrict__ out_T,
                                          uint32_t* __restrict__ out_last, const float* __restrict__ target,
@@ -260,7 +272,6 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
     c22[q] = f2_make(c2[2 * q], c2[2 * q + 1]);
     fy2[q] = f2_make(fy[2 * q], fy[2 * q + 1]);
   }
-  const f2 fx2 = f2_dup(fx);
   // centres of the slab's first and last rows (the same for every lane)
   const float fy_first = float(py0) + 0.5f, fy_last = float(py0 + G::SLAB_ROWS - 1) + 0.5f;
   const uint32_t inside = live;
@@ -277,18 +288,22 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
     if (live) {
       for (int j = 0; j < k_staged; ++j) {
         const float4 ee = sm[j].e;
-        if (!(ee.z <= fx && fx <= ee.w)) continue;
-        const ulonglong2 qa = *reinterpret_cast<const ulonglong2*>(&sm[j].a);  // (px,px) (py,py)
-        const ulonglong2 qb = *reinterpret_cast<const ulonglong2*>(&sm[j].b);  // (kA,kA) (k2B,k2B)
-        const ulonglong2 qc = *reinterpret_cast<const ulonglong2*>(&sm[j].c);  // (kC,kC) (op,op)
-        const ulonglong2 qd = *reinterpret_cast<const ulonglong2*>(&sm[j].d);  // (r,r) (g,g)
-        const f2 qbl = *reinterpret_cast<const f2*>(&sm[j].e);                  // (b,b)
-        const float4 ef = sm[j].f;
-        const f2 dx2 = sub2(fx2, qa.x);
-        const f2 kadxdx2 = mul2(mul2(qb.x, dx2), dx2);
-        const f2 kb2dx2 = mul2(qb.y, dx2);
-        const uint32_t pos = __float_as_uint(ef.w);
-        // all instances compute the same bits: `inrange` skips the exponent
+        if (!(ee.x <= fx && fx <= ee.y)) continue;
+        const ulonglong2 qa = *reinterpret_cast<const ulonglong2*>(&sm[j].a);  // (py,py) (2B,2B)
+        const ulonglong2 qb = *reinterpret_cast<const ulonglong2*>(&sm[j].b);  // (C,C) (op,op)
+        const ulonglong2 qc = *reinterpret_cast<const ulonglong2*>(&sm[j].c);  // (r,r) (g,g)
+        const float4 ed = sm[j].d;                                             // b, b, px, A
+        const f2 qbl = f2_make(ed.x, ed.y);
+        const float2 ef = *reinterpret_cast<const float2*>(&sm[j].f);
+        // q = A dx dx + B (dx dy + dy dx) + C dy dy in the reference's
+        // order (mat2_sym::mult_vec_from_both_sides); dx is fixed per lane,
+        // so (A dx) dx is formed once per entry, and B (dx dy + dy dx) is
+        // (2B)(dx dy) exactly
+        const float dx = fs(fx, ed.z);
+        const f2 adxdx2 = f2_dup(fm(fm(ed.w, dx), dx));
+        const f2 dx2 = f2_dup(dx);
+        const uint32_t pos = __float_as_uint(ef.y);
+        // all instances compute the same bits: `inrange` skips expf_cr's
         // range check (proven by the entry's staged flag), `rows` the row
         // test of an entry whose box holds every row of the slab
         auto blend_slots = [&](auto inrange, auto rows) {
@@ -297,33 +312,33 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
             // a slot is one row of the slab across the warp: the skips are
             // warp-uniform in practice
             const int k0 = 2 * q, k1 = 2 * q + 1;
-            const bool a0 = ((live >> k0) & 1u) && (decltype(rows)::value || (ef.x <= fy[k0] && fy[k0] <= ef.y));
-            const bool a1 = ((live >> k1) & 1u) && (decltype(rows)::value || (ef.x <= fy[k1] && fy[k1] <= ef.y));
+            const bool a0 = ((live >> k0) & 1u) && (decltype(rows)::value || (ee.z <= fy[k0] && fy[k0] <= ee.w));
+            const bool a1 = ((live >> k1) & 1u) && (decltype(rows)::value || (ee.z <= fy[k1] && fy[k1] <= ee.w));
             if (!(a0 || a1)) continue;
-            const f2 dy2 = sub2(fy2[q], qa.y);
-            const f2 y2 = fma2(fma2(qc.x, dy2, kb2dx2), dy2, kadxdx2);
-            const f2 ex2v = decltype(inrange)::value ? exp2_det2_inrange(y2) : exp2_det2(y2);
+            const f2 dy2 = sub2(fy2[q], qa.x);
+            const f2 qf = add2(add2(adxdx2, mul2(qa.y, mul2(dx2, dy2))), mul2(mul2(qb.x, dy2), dy2));
+            const f2 g2 = expf_cr2<!decltype(inrange)::value>(mul2(qf, f2_dup(-0.5f)), tab);
+            const f2 al = mul2(g2, qb.y);
             // an inactive slot of the pair takes alpha 0: its state is unchanged
-            const f2 e2 = f2_make(a0 ? f2_lo(ex2v) : 0.f, a1 ? f2_hi(ex2v) : 0.f);
-            const f2 al2 = mul2(e2, qc.y);
-            const f2 eo2 = mul2(T2[q], al2);
-            c02[q] = fma2(qd.x, eo2, c02[q]);
-            c12[q] = fma2(qd.y, eo2, c12[q]);
-            c22[q] = fma2(qbl, eo2, c22[q]);
-            T2[q] = sub2(T2[q], eo2);
+            const f2 e2 = f2_make(a0 ? f2_lo(al) : 0.f, a1 ? f2_hi(al) : 0.f);
+            const f2 eo2 = mul2(T2[q], e2);
+            c02[q] = add2(c02[q], mul2(qc.x, eo2));
+            c12[q] = add2(c12[q], mul2(qc.y, eo2));
+            c22[q] = add2(c22[q], mul2(qbl, eo2));
+            T2[q] = mul2(T2[q], sub2(f2_dup(1.f), e2));
             as2[q] = add2(as2[q], eo2);
-            if (a0 && f2_lo(as2[q]) >= kAlphaBreak) {
+            if (a0 && (CUDA_STOP ? f2_lo(as2[q]) >= kAlphaStop : f2_lo(as2[q]) > kAlphaStop)) {
               live &= ~(1u << k0);
               last[k0] = pos;
             }
-            if (a1 && f2_hi(as2[q]) >= kAlphaBreak) {
+            if (a1 && (CUDA_STOP ? f2_hi(as2[q]) >= kAlphaStop : f2_hi(as2[q]) > kAlphaStop)) {
               live &= ~(1u << k1);
               last[k1] = pos;
             }
           }
         };
-        const bool all_rows = ef.x <= fy_first && fy_last <= ef.y;
-        if (__float_as_uint(ef.z)) {
+        const bool all_rows = ee.z <= fy_first && fy_last <= ee.w;
+        if (__float_as_uint(ef.x)) {
           if (all_rows)
             blend_slots(std::true_type{}, std::true_type{});
           else
@@ -379,6 +394,13 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
   return e - hi;
 }
 
+// Copies expf_cr's 2^(j/64) table into the block's shared memory (one
+// barrier, at kernel start).
+__device__ __forceinline__ void load_exp_table(float2* tab) {
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) tab[i] = g_exp2_64[i];
+  __syncthreads();
+}
+
 // The superblock-list range of an item and the tile's place in it.
 struct ItemGeo {
   int v, px0, py0;
@@ -417,6 +439,8 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     float* __restrict__ slab_loss, uint32_t* __restrict__ item_cost) {
   using G = TaskGeo<TS, PPL, NT>;
   __shared__ EntP sm_all[kRasterWarps][32];
+  __shared__ float2 tab[64];
+  load_exp_table(tab);
   EntP* sm = sm_all[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const uint32_t num_tasks = b.num_items * G::SLABS;
@@ -440,8 +464,8 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     PackedSrc src{rec + 3 * size_t(ig.v) * n};
     SbWalkSpan walk{list1, ig.lx, ig.ly, nx};
     const int xend = min(vd.w, ig.px0 + int(nx) * TS);
-    const uint32_t walked = fwd_slab<G::GX, G::PPL>(
-        walk, src, sm, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, xend, false, out_rgb,
+    const uint32_t walked = fwd_slab<G::GX, G::PPL, false>(
+        walk, src, sm, tab, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, xend, false, out_rgb,
         vd.pix_base, out_T, out_last, target, grad_pix, slab_loss ? slab_loss + size_t(item) * G::SLABS + slab : nullptr);
     // scheduling hint for the backward and the next forward: list positions walked
     if (lane == 0 && walked) atomicMax(&item_cost[item], walked);
@@ -451,13 +475,15 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
 
 // Drop-in forward (splat_gauss.rs:46-94): AoS inputs and per-tile lists,
 // accumulates into pix2rgb.
-template <int TS, int PPL>
+template <int TS, int PPL, bool CUDA_STOP>
 __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
     int w, int h, int tile_w, uint32_t num_tasks, float* __restrict__ pix2rgb, AosSrc src,
     const uint32_t* __restrict__ tile2idx, const uint32_t* __restrict__ idx2pnt, float* __restrict__ out_T,
     uint32_t* __restrict__ out_last) {
   using G = Geo<TS, PPL>;
   __shared__ EntP sm_all[kRasterWarps][32];
+  __shared__ float2 tab[64];
+  load_exp_table(tab);
   EntP* sm = sm_all[threadIdx.x >> 5];
   const uint32_t task = blockIdx.x * kRasterWarps + (threadIdx.x >> 5);
   if (task >= num_tasks) return;
@@ -465,7 +491,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
   const int px0 = int(tile % uint32_t(tile_w)) * TS;
   const int py0 = int(tile / uint32_t(tile_w)) * TS + int(slab) * G::SLAB_ROWS;
   TileWalk walk{idx2pnt};
-  fwd_slab<TS, PPL>(walk, src, sm, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, w, true, pix2rgb, 0, out_T,
+  fwd_slab<TS, PPL, CUDA_STOP>(walk, src, sm, tab, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, w, true, pix2rgb, 0, out_T,
                     out_last, nullptr, nullptr, nullptr);
 }
 
@@ -771,35 +797,57 @@ cudaError_t raster_bwd(cudaStream_t st, const ViewBatch& b, const BwdArgs& a) {
   return cudaErrorInvalidValue;
 }
 
-template <int TS, int PPL>
+template <int TS, int PPL, bool CUDA_STOP>
 static void launch_aos(cudaStream_t st, int w, int h, float* pix2rgb, const AosSrc& src, const uint32_t* tile2idx,
                        const uint32_t* idx2pnt, float* out_T, uint32_t* out_last) {
   const int tw = (w + TS - 1) / TS, th = (h + TS - 1) / TS;
   const uint32_t tasks = uint32_t(tw) * uint32_t(th) * Geo<TS, PPL>::SLABS;
   const unsigned grid = (tasks + kRasterWarps - 1) / kRasterWarps;
-  k_raster_fwd_aos<TS, PPL><<<grid, 32 * kRasterWarps, 0, st>>>(w, h, tw, tasks, pix2rgb, src, tile2idx, idx2pnt,
-                                                                out_T, out_last);
+  k_raster_fwd_aos<TS, PPL, CUDA_STOP><<<grid, 32 * kRasterWarps, 0, st>>>(w, h, tw, tasks, pix2rgb, src, tile2idx,
+                                                                           idx2pnt, out_T, out_last);
   count_launch();
 }
 
-cudaError_t raster_fwd_aos(cudaStream_t st, int ts, int w, int h, float* pix2rgb, const float* xyd, const float* conic,
-                           const float* aabb, const float* opacity, const float* rgb, const uint32_t* tile2idx,
-                           const uint32_t* idx2pnt, float* out_T, uint32_t* out_last) {
-  if (w <= 0 || h <= 0) return cudaSuccess;
-  const AosSrc src{xyd, conic, aabb, opacity, rgb};
+template <bool CUDA_STOP>
+static cudaError_t launch_aos_ts(cudaStream_t st, int ts, int w, int h, float* pix2rgb, const AosSrc& src,
+                                 const uint32_t* tile2idx, const uint32_t* idx2pnt, float* out_T,
+                                 uint32_t* out_last) {
   switch (ts) {
     case 8:
-      launch_aos<8, 2>(st, w, h, pix2rgb, src, tile2idx, idx2pnt, out_T, out_last);
+      launch_aos<8, 2, CUDA_STOP>(st, w, h, pix2rgb, src, tile2idx, idx2pnt, out_T, out_last);
       break;
     case 16:
-      launch_aos<16, 4>(st, w, h, pix2rgb, src, tile2idx, idx2pnt, out_T, out_last);
+      launch_aos<16, 4, CUDA_STOP>(st, w, h, pix2rgb, src, tile2idx, idx2pnt, out_T, out_last);
       break;
     case 32:
-      launch_aos<32, 4>(st, w, h, pix2rgb, src, tile2idx, idx2pnt, out_T, out_last);
+      launch_aos<32, 4, CUDA_STOP>(st, w, h, pix2rgb, src, tile2idx, idx2pnt, out_T, out_last);
       break;
     default:
       return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t raster_fwd_aos(cudaStream_t st, int ts, int w, int h, float* pix2rgb, const float* xyd, const float* conic,
+                           const float* aabb, const float* opacity, const float* rgb, const uint32_t* tile2idx,
+                           const uint32_t* idx2pnt, float* out_T, uint32_t* out_last, bool cuda_stop) {
+  if (w <= 0 || h <= 0) return cudaSuccess;
+  const AosSrc src{xyd, conic, aabb, opacity, rgb};
+  return cuda_stop ? launch_aos_ts<true>(st, ts, w, h, pix2rgb, src, tile2idx, idx2pnt, out_T, out_last)
+                   : launch_aos_ts<false>(st, ts, w, h, pix2rgb, src, tile2idx, idx2pnt, out_T, out_last);
+}
+
+// expf_cr elementwise (exposed so that it can be checked against a
+// correctly rounded reference on every float).
+__global__ void k_expf_cr(size_t n, const float* __restrict__ x, float* __restrict__ y) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = expf_cr(x[i]);
+}
+
+cudaError_t expf_cr_launch(cudaStream_t st, size_t n, const float* x, float* y) {
+  if (n == 0) return cudaSuccess;
+  k_expf_cr<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, x, y);
+  count_launch();
   return cudaGetLastError();
 }
 

@@ -13,6 +13,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libdsplat.so")
 
 DSPLAT_OK = 0
+STOP_CPU = 0   # del-splat-cpu's stop test, alpha_sum > 0.999f
+STOP_CUDA = 1  # the reference CUDA kernel's, alpha_sum > 0.999 in double
 ERRORS = {1: "invalid argument", 2: "pair capacity exceeded", 3: "CUDA error", 4: "workspace too small",
           5: "unsupported"}
 
@@ -67,6 +69,9 @@ SIGNATURES = {
     "dsplat_gauss_tile2idx_count": (c_i32, [_P, c_u32, _P, c_u32, c_u32, c_u32, _P, c_size, ctypes.POINTER(c_u64)]),
     "dsplat_gauss_tile2idx_idx2pnt": (c_i32, [_P, c_u32, _P, _P, c_u32, c_u32, c_u32, _P, _P, c_u64, _P, _P, c_size]),
     "dsplat_gauss_rasterize_pnt2splat2": (c_i32, [_P, c_u32, c_u32, _P, _P, _P, _P, _P, _P, c_u32, _P, _P, _P, _P]),
+    "dsplat_gauss_rasterize_pnt2splat2_stop": (c_i32, [_P, c_u32, c_u32, _P, _P, _P, _P, _P, _P, c_u32, _P, _P, _P,
+                                                       _P, c_i32]),
+    "dsplat_expf_cr": (c_i32, [_P, c_u64, _P, _P]),
     "dsplat_circle_pnt2splat3_to_pnt2splat2": (c_i32, [_P, c_u32, _P, _P, _P, _P, c_u32, c_u32, c_f32]),
     "dsplat_circle_tile2idx_count": (c_i32, [_P, c_u32, _P, _P, c_u32, c_u32, c_u32, _P, c_size,
                                              ctypes.POINTER(c_u64)]),

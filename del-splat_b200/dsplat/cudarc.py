@@ -102,20 +102,30 @@ def splat_gauss_tile2idx_idx2pnt(stream, img_shape, tile_size, pnt2pixxydepth, p
 
 def splat_gauss_rasterize_pnt2splat2(stream, img_shape, pix2rgb, pnt2pixxydepth, pnt2pixconvinv, pnt2pixaabb,
                                      pnt2opacity, pnt2rgb, tile_size, tile2idx, idx2pnt, pix2transmit=None,
-                                     pix2stop=None) -> None:
+                                     pix2stop=None, stop_rule: int = N.STOP_CPU) -> None:
+    """Adds the tiled front-to-back blend into pix2rgb.  stop_rule: N.STOP_CPU
+    (del-splat-cpu, alpha_sum > 0.999f, the default) or N.STOP_CUDA (the
+    reference CUDA kernel's double comparison)."""
     n = pnt2pixxydepth.numel() // 3
     w, h = int(img_shape[0]), int(img_shape[1])
     tw, th = tile_shape(img_shape, tile_size)
     if tile2idx.numel() != tw * th + 1:
         raise ValueError(f"tile2idx: expected {tw * th + 1} entries, got {tile2idx.numel()}")
-    N.check(N.lib().dsplat_gauss_rasterize_pnt2splat2(
+    N.check(N.lib().dsplat_gauss_rasterize_pnt2splat2_stop(
         _st(stream, pix2rgb.device), w, h, _chk(pix2rgb, "pix2rgb", w * h * 3),
         _chk(pnt2pixxydepth, "pnt2pixxydepth", 3 * n), _chk(pnt2pixconvinv, "pnt2pixconvinv", 3 * n),
         _chk(pnt2pixaabb, "pnt2pixaabb", 4 * n), _chk(pnt2opacity, "pnt2opacity", n), _chk(pnt2rgb, "pnt2rgb", 3 * n),
         int(tile_size), _chk(tile2idx, "tile2idx", dtype=tile2idx.dtype), _chk(idx2pnt, "idx2pnt", dtype=idx2pnt.dtype),
         _chk(pix2transmit, "pix2transmit", w * h) if pix2transmit is not None else None,
-        _chk(pix2stop, "pix2stop", w * h, dtype=pix2stop.dtype) if pix2stop is not None else None),
+        _chk(pix2stop, "pix2stop", w * h, dtype=pix2stop.dtype) if pix2stop is not None else None, int(stop_rule)),
         "rasterize_pnt2splat2")
+
+
+def expf_cr(x: torch.Tensor, stream=None) -> torch.Tensor:
+    """The blend's exponential: e^x correctly rounded to float32, elementwise."""
+    y = torch.empty_like(x)
+    N.check(N.lib().dsplat_expf_cr(_st(stream, x.device), x.numel(), _chk(x, "x"), y.data_ptr()), "expf_cr")
+    return y
 
 
 def splat_circle_pnt2splat3_to_pnt2splat2(stream, pnt2xyz, pnt2pixxydepth, pnt2pixrad, transform_world2ndc,

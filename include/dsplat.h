@@ -72,12 +72,32 @@ int dsplat_gauss_tile2idx_idx2pnt(dsplat_stream stream, uint32_t num_pnt, const 
 /* del-splat-cudarc/src/splat_gauss.rs:46-94 rasterize_pnt2splat2 (kernel
  * splat_gauss.cu:56-109): accumulates into pix2rgb like the reference.
  * pix2transmit [H,W] and pix2stop [H,W] (nullable) receive the final
- * transmittance and the list position where each pixel's walk stopped. */
+ * transmittance and the list position where each pixel's walk stopped.
+ * The blend performs del-splat-cpu's f32 operations (pnt2pixxyndcz.rs:86-93)
+ * with a correctly rounded exp and its stop test alpha_sum > 0.999f. */
 int dsplat_gauss_rasterize_pnt2splat2(dsplat_stream stream, uint32_t img_w, uint32_t img_h, float* pix2rgb,
                                       const float* pnt2pixxydepth, const float* pnt2pixconvinv,
                                       const float* pnt2pixaabb, const float* pnt2opacity, const float* pnt2rgb,
                                       uint32_t tile_size, const uint32_t* tile2idx, const uint32_t* idx2pnt,
                                       float* pix2transmit, uint32_t* pix2stop);
+
+/* The same with a choice of stop test: DSPLAT_STOP_CPU is del-splat-cpu's
+ * (pnt2pixxyndcz.rs:93, f32 alpha_sum > 0.999f), DSPLAT_STOP_CUDA the
+ * reference CUDA kernel's (splat_gauss.cu:105, `alpha_sum > 0.999` in double,
+ * i.e. alpha_sum >= 0.999f).  The two reference paths disagree exactly when
+ * a pixel's sum lands on 0.999f. */
+#define DSPLAT_STOP_CPU 0
+#define DSPLAT_STOP_CUDA 1
+int dsplat_gauss_rasterize_pnt2splat2_stop(dsplat_stream stream, uint32_t img_w, uint32_t img_h, float* pix2rgb,
+                                           const float* pnt2pixxydepth, const float* pnt2pixconvinv,
+                                           const float* pnt2pixaabb, const float* pnt2opacity, const float* pnt2rgb,
+                                           uint32_t tile_size, const uint32_t* tile2idx, const uint32_t* idx2pnt,
+                                           float* pix2transmit, uint32_t* pix2stop, int32_t stop_rule);
+
+/* No reference counterpart: the blend's exponential, y[i] = e^x[i]
+ * correctly rounded to float (the exp that del-splat-cpu's f32 `exp` call
+ * approximates to within one unit in the last place), elementwise. */
+int dsplat_expf_cr(dsplat_stream stream, uint64_t n, const float* x, float* y);
 
 /* ===================== del-splat-cudarc :: splat_circle ================= */
 

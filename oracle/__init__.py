@@ -6,13 +6,22 @@ import this package.  It wraps two shared libraries with ctypes:
 * ``oracle/_build/liboracle.so`` -- the C++ restatement (oracle/oracle.cpp) of
   del-splat-cpu and the reference CUDA kernels, plus an FP64 gradient oracle.
 * ``oracle/_ref/libdsplat_ref.so`` -- the reference's own
-  ``tile_acceleration.h`` and ``splat_point.cu`` compiled as host C++
-  (oracle/ref/), used to pin the restatement.  Present only when it was built
-  from a del-splat checkout; ``ref_available()`` says whether it is.
+  ``tile_acceleration.h``, ``splat_point.cu``, ``splat_gauss.cu`` and
+  ``splat_circle.cu`` compiled as host C++ (oracle/ref/), used to pin the
+  restatement.  Present only when it was built from a del-splat checkout;
+  ``ref_available()`` says whether it is.
 
-Parity status: tile spans, key bits and the point z-buffer are pinned against
-the reference's own code; the projection maths (absent del-geo crate) is a
+Parity status: tile spans, key bits, the point z-buffer, the blend (with the
+C library's expf and the kernel's double stop test) and the way the
+reference's kernels compose the del-geo helpers are pinned against the
+reference's own code; the del-geo helpers themselves (absent crate) are a
 restatement whose parity with upstream is unpinned.
+
+Blend modes (``mode`` arguments): 0 is the product's arithmetic -- del-splat-
+cpu's f32 operations with a correctly rounded exp and the f32 stop test
+``alpha_sum > 0.999f``; ``BLEND_LIBM_EXP`` uses the C library's expf (what
+del-splat-cpu's ``f32::exp`` calls), ``BLEND_CUDA_STOP`` the CUDA kernel's
+double stop test (``alpha_sum >= 0.999f``).
 """
 from __future__ import annotations
 
@@ -40,11 +49,16 @@ _i64 = ctypes.c_int64
 _int = ctypes.c_int
 
 
+BLEND_LIBM_EXP = 1
+BLEND_CUDA_STOP = 2
+
+
 def build(reference_root: Optional[str] = None) -> None:
-    """Compile the oracle (and, if the reference tree is present, the pin)."""
+    """Compile the oracle, and the pin when ``reference_root`` (or the
+    DSPLAT_REFERENCE_ROOT environment variable) names a del-splat checkout."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
-    ref = reference_root or "/root/reference"
-    if os.path.isdir(os.path.join(ref, "del-splat-cuda-kernels")):
+    ref = reference_root or os.environ.get("DSPLAT_REFERENCE_ROOT")
+    if ref and os.path.isdir(os.path.join(ref, "del-splat-cuda-kernels")):
         subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "ref"), f"REF={ref}"], check=True)
 
 
@@ -72,6 +86,15 @@ def ref() -> ctypes.CDLL:
         _ref.ref_tiles_fill.argtypes = [_i64, _f32p, _f32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p, _u64p]
         _ref.ref_point_zbuffer.restype = None
         _ref.ref_point_zbuffer.argtypes = [ctypes.c_uint32, _f32p, _f32p, _f32p, _f32p, _int, _int]
+        u32 = ctypes.c_uint32
+        _ref.ref_gauss_project.restype = None
+        _ref.ref_gauss_project.argtypes = [u32, _f32p, _f32p, _f32p, _f32p, u32, u32, _f32p, _f32p, _f32p]
+        _ref.ref_gauss_rasterize.restype = None
+        _ref.ref_gauss_rasterize.argtypes = [u32, u32, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, u32, _u32p, _u32p]
+        _ref.ref_circle_project.restype = None
+        _ref.ref_circle_project.argtypes = [u32, _f32p, _f32p, u32, u32, ctypes.c_float, _f32p, _f32p]
+        _ref.ref_circle_rasterize.restype = None
+        _ref.ref_circle_rasterize.argtypes = [u32, u32, _f32p, u32, _u32p, _u32p, _f32p, _f32p, _f32p]
     return _ref
 
 
@@ -95,13 +118,16 @@ def _declare(L: ctypes.CDLL) -> None:
         "orc_tile2pnt_fill": (None, [_i64, _f32p, _f32p, _int, _int, _int, _u32p, _u32p, _u64p]),
         "orc_gauss_rasterize_tiled": (None, [_int, _int, _int, _u32p, _u32p, _f32p, _f32p, _f32p, _f32p, _f32p,
                                              _f32p, _f32p, _i32p, _int]),
+        "orc_gauss_rasterize_tiled_mode": (None, [_int, _int, _int, _u32p, _u32p, _f32p, _f32p, _f32p, _f32p,
+                                                  _f32p, _f32p, _f32p, _i32p, _int, _int]),
         "orc_gauss_render_naive": (None, [_i64, _f32p, _f32p, _f32p, _f32p, _f32p, _int, _int, _f32p]),
+        "orc_gauss_render_naive_mode": (None, [_i64, _f32p, _f32p, _f32p, _f32p, _f32p, _int, _int, _f32p, _int]),
         "orc_circle_splat_tiled": (None, [_int, _int, _int, _u32p, _u32p, _f32p, _f32p, _i32p]),
         "orc_point_render_sort_depth": (None, [_i64, _f32p, _int, _int, _i32p]),
         "orc_fused_project": (None, [_i64, _f32p, _f32p, _f32p, _f32p, _int, _f32p, _f32p, _int, _int,
                                      _f32p, _f32p, _f32p, _f32p]),
         "orc_sh_eval": (None, [_i64, _f32p, _f32p, _int, _f32p, _f32p]),
-        "orc_exp2_det": (None, [_i64, _f32p, _f32p]),
+        "orc_expf_cr": (None, [_i64, _f32p, _f32p]),
         "orc64_loss": (ctypes.c_double, [ctypes.POINTER(Scene64), _u8p, _f64p]),
         "orc64_backward": (ctypes.c_double, [ctypes.POINTER(Scene64), _f64p, _f64p, _f64p, _f64p, _f64p]),
         "orc64_fd": (ctypes.c_double, [ctypes.POINTER(Scene64), _int, _i64, _int, ctypes.c_double]),
@@ -124,11 +150,11 @@ def f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
-def exp2_det(y):
-    """The blend's deterministic 2^y (exp2_det), elementwise."""
-    y = f32(y).ravel()
-    out = np.empty_like(y)
-    lib().orc_exp2_det(y.size, _p(y, _f32p), _p(out, _f32p))
+def expf_cr(x):
+    """exp(x) correctly rounded to float32, elementwise (threaded)."""
+    x = f32(x).ravel()
+    out = np.empty_like(x)
+    lib().orc_expf_cr(x.size, _p(x, _f32p), _p(out, _f32p))
     return out
 
 
@@ -192,24 +218,26 @@ def tile2pnt(xyd, aabb, w, h, ts, with_keys=True):
     return tile2idx, idx2pnt, keys
 
 
-def gauss_rasterize_tiled(w, h, ts, tile2idx, idx2pnt, xyd, conic, aabb, opacity, rgb, nthreads=1):
+def gauss_rasterize_tiled(w, h, ts, tile2idx, idx2pnt, xyd, conic, aabb, opacity, rgb, nthreads=1, mode=0):
+    """Tiled front-to-back blend -> (image [H,W,3], final T [H,W], stop position [H,W])."""
     pix = np.zeros((h, w, 3), np.float32)
     T = np.zeros((h, w), np.float32)
     last = np.zeros((h, w), np.int32)
     tile2idx = np.ascontiguousarray(tile2idx, np.uint32)
     idx2pnt = np.ascontiguousarray(idx2pnt, np.uint32)
     xyd, conic, aabb, opacity, rgb = f32(xyd), f32(conic), f32(aabb), f32(opacity), f32(rgb)
-    lib().orc_gauss_rasterize_tiled(w, h, ts, _p(tile2idx, _u32p), _p(idx2pnt, _u32p), _p(xyd, _f32p),
-                                    _p(conic, _f32p), _p(aabb, _f32p), _p(opacity, _f32p), _p(rgb, _f32p),
-                                    _p(pix, _f32p), _p(T, _f32p), _p(last, _i32p), nthreads)
+    lib().orc_gauss_rasterize_tiled_mode(w, h, ts, _p(tile2idx, _u32p), _p(idx2pnt, _u32p), _p(xyd, _f32p),
+                                         _p(conic, _f32p), _p(aabb, _f32p), _p(opacity, _f32p), _p(rgb, _f32p),
+                                         _p(pix, _f32p), _p(T, _f32p), _p(last, _i32p), nthreads, int(mode))
     return pix, T, last
 
 
-def gauss_render_naive(xyd, conic, aabb, opacity, rgb, w, h):
+def gauss_render_naive(xyd, conic, aabb, opacity, rgb, w, h, mode=0):
+    """pnt2pixxyndcz.rs:42-100 (untiled, global depth order)."""
     xyd, conic, aabb, opacity, rgb = f32(xyd), f32(conic), f32(aabb), f32(opacity), f32(rgb)
     pix = np.zeros((h, w, 3), np.float32)
-    lib().orc_gauss_render_naive(xyd.shape[0], _p(xyd, _f32p), _p(conic, _f32p), _p(aabb, _f32p),
-                                 _p(opacity, _f32p), _p(rgb, _f32p), w, h, _p(pix, _f32p))
+    lib().orc_gauss_render_naive_mode(xyd.shape[0], _p(xyd, _f32p), _p(conic, _f32p), _p(aabb, _f32p),
+                                      _p(opacity, _f32p), _p(rgb, _f32p), w, h, _p(pix, _f32p), int(mode))
     return pix
 
 
@@ -304,3 +332,48 @@ def ref_point_zbuffer(xyd, rgb, w, h):
     img = np.zeros((h, w, 3), np.float32)
     ref().ref_point_zbuffer(xyd.shape[0], _p(xyd, _f32p), _p(rgb, _f32p), _p(depth, _f32p), _p(img, _f32p), w, h)
     return depth, img
+
+
+def ref_gauss_project(xyz, quat, scale, mvp, w, h):
+    """The reference's splat_gauss.cu:10-53 run on the CPU (del-geo restated)."""
+    xyz, quat, scale, mvp = f32(xyz), f32(quat), f32(scale), f32(mvp).reshape(16)
+    n = xyz.shape[0]
+    xyd = np.zeros((n, 3), np.float32)
+    conic = np.zeros((n, 3), np.float32)
+    aabb = np.zeros((n, 4), np.float32)
+    ref().ref_gauss_project(n, _p(xyz, _f32p), _p(quat, _f32p), _p(scale, _f32p), _p(mvp, _f32p), w, h,
+                            _p(xyd, _f32p), _p(conic, _f32p), _p(aabb, _f32p))
+    return xyd, conic, aabb
+
+
+def ref_gauss_rasterize(w, h, ts, tile2idx, idx2pnt, xyd, conic, aabb, opacity, rgb):
+    """The reference's splat_gauss.cu:56-109 run on the CPU -> image [H,W,3]."""
+    pix = np.zeros((h, w, 3), np.float32)
+    tile2idx = np.ascontiguousarray(tile2idx, np.uint32)
+    idx2pnt = np.ascontiguousarray(idx2pnt, np.uint32)
+    xyd, conic, aabb, opacity, rgb = f32(xyd), f32(conic), f32(aabb), f32(opacity), f32(rgb)
+    ref().ref_gauss_rasterize(w, h, _p(pix, _f32p), _p(xyd, _f32p), _p(conic, _f32p), _p(aabb, _f32p),
+                              _p(opacity, _f32p), _p(rgb, _f32p), ts, _p(tile2idx, _u32p), _p(idx2pnt, _u32p))
+    return pix
+
+
+def ref_circle_project(xyz, mvp, w, h, radius):
+    """The reference's splat_circle.cu:7-41 run on the CPU."""
+    xyz, mvp = f32(xyz), f32(mvp).reshape(16)
+    n = xyz.shape[0]
+    xyd = np.zeros((n, 3), np.float32)
+    rad = np.zeros((n,), np.float32)
+    ref().ref_circle_project(n, _p(xyz, _f32p), _p(mvp, _f32p), w, h, float(radius), _p(xyd, _f32p),
+                             _p(rad, _f32p))
+    return xyd, rad
+
+
+def ref_circle_rasterize(w, h, ts, tile2idx, idx2pnt, xyd, rad, rgb):
+    """The reference's splat_circle.cu:93-132 run on the CPU -> image [H,W,3]."""
+    pix = np.zeros((h, w, 3), np.float32)
+    tile2idx = np.ascontiguousarray(tile2idx, np.uint32)
+    idx2pnt = np.ascontiguousarray(idx2pnt, np.uint32)
+    xyd, rad, rgb = f32(xyd), f32(rad), f32(rgb)
+    ref().ref_circle_rasterize(w, h, _p(pix, _f32p), ts, _p(tile2idx, _u32p), _p(idx2pnt, _u32p),
+                               _p(xyd, _f32p), _p(rad, _f32p), _p(rgb, _f32p))
+    return pix

@@ -28,6 +28,7 @@
 // from their mathematical definitions (the crate is unpinned upstream: path
 // dependency ../del-geo, deploy pins 0.1.32/0.1.33 commented out).
 #include "oracle.h"
+#include "del_geo_restated.h"
 
 #include <algorithm>
 #include <parallel/algorithm>
@@ -41,121 +42,7 @@
 
 namespace {
 
-// ----------------------------------------------------------------------------
-// del-geo restatements.  M is a column-major 4x4 (M[i + 4*j] = row i, col j).
-// ----------------------------------------------------------------------------
-template <class T>
-inline void transform_homogeneous(const T* m, const T* p, T* out) {
-  T x = m[0] * p[0] + m[4] * p[1] + m[8] * p[2] + m[12];
-  T y = m[1] * p[0] + m[5] * p[1] + m[9] * p[2] + m[13];
-  T z = m[2] * p[0] + m[6] * p[1] + m[10] * p[2] + m[14];
-  T w = m[3] * p[0] + m[7] * p[1] + m[11] * p[2] + m[15];
-  out[0] = x / w;
-  out[1] = y / w;
-  out[2] = z / w;
-}
-
-// d(transform_homogeneous)/dp, 3x3 column-major: J[i + 3*j] = d ndc_i / d p_j.
-template <class T>
-inline void jacobian_transform(const T* t, const T* p, T* J) {
-  T a[3];
-  a[0] = t[0] * p[0] + t[4] * p[1] + t[8] * p[2] + t[12];
-  a[1] = t[1] * p[0] + t[5] * p[1] + t[9] * p[2] + t[13];
-  a[2] = t[2] * p[0] + t[6] * p[1] + t[10] * p[2] + t[14];
-  T b = t[3] * p[0] + t[7] * p[1] + t[11] * p[2] + t[15];
-  T ee = T(1) / b;
-  T ee2 = ee * ee;
-  for (int j = 0; j < 3; ++j)
-    for (int i = 0; i < 3; ++i)
-      J[i + 3 * j] = t[i + 4 * j] * ee - a[i] * t[3 + 4 * j] * ee2;
-}
-
-// ndc -> pixel as a 2x3 column-major affine map (third column = translation).
-template <class T>
-inline void transform_ndc2pix(int w, int h, T* n) {
-  n[0] = T(0.5) * T(w);
-  n[1] = T(0);
-  n[2] = T(0);
-  n[3] = T(-0.5) * T(h);
-  n[4] = T(0.5) * T(w);
-  n[5] = T(0.5) * T(h);
-}
-
-// (2x3) * (3x3), column-major.  Used with the ndc->pixel map exactly as the
-// reference composes it (splat_gauss.cu:28), i.e. including the third column.
-template <class T>
-inline void mult_2x3_3x3(const T* a, const T* b, T* r) {
-  for (int j = 0; j < 3; ++j)
-    for (int i = 0; i < 2; ++i)
-      r[i + 2 * j] = a[i] * b[0 + 3 * j] + a[i + 2] * b[1 + 3 * j] +
-                     a[i + 4] * b[2 + 3 * j];
-}
-
-// unit quaternion (x, y, z, w) -> 3x3 rotation, column-major.
-template <class T>
-inline void quat_to_mat3(const T* q, T* r) {
-  T x2 = q[0] * q[0] * T(2), y2 = q[1] * q[1] * T(2), z2 = q[2] * q[2] * T(2);
-  T xy = q[0] * q[1] * T(2), yz = q[1] * q[2] * T(2), zx = q[2] * q[0] * T(2);
-  T xw = q[0] * q[3] * T(2), yw = q[1] * q[3] * T(2), zw = q[2] * q[3] * T(2);
-  r[0] = T(1) - y2 - z2; r[1] = xy + zw;          r[2] = zx - yw;
-  r[3] = xy - zw;          r[4] = T(1) - z2 - x2; r[5] = yz + xw;
-  r[6] = zx + yw;          r[7] = yz - xw;          r[8] = T(1) - x2 - y2;
-}
-
-// symmetric 2x2 (a, b, c) = P R diag(d)^2 R^T P^T
-template <class T>
-inline void projected_spd_mat3(const T* p, const T* q, const T* d, T* abc) {
-  T r[9], pr[6];
-  quat_to_mat3(q, r);
-  mult_2x3_3x3(p, r, pr);
-  T dd0 = d[0] * d[0], dd1 = d[1] * d[1], dd2 = d[2] * d[2];
-  abc[0] = pr[0] * pr[0] * dd0 + pr[2] * pr[2] * dd1 + pr[4] * pr[4] * dd2;
-  abc[1] = pr[0] * pr[1] * dd0 + pr[2] * pr[3] * dd1 + pr[4] * pr[5] * dd2;
-  abc[2] = pr[1] * pr[1] * dd0 + pr[3] * pr[3] * dd1 + pr[5] * pr[5] * dd2;
-}
-
-// Inverse of a symmetric 2x2 whose eigenvalues are clamped from below at eps.
-// Only +, -, *, /, sqrt are used so that the GPU can reproduce it exactly.
-template <class T>
-inline void safe_inverse_spd(const T* s, T eps, T* inv) {
-  T a = s[0], b = s[1], c = s[2];
-  T hm = (a + c) * T(0.5);
-  T hd = (a - c) * T(0.5);
-  T r = std::sqrt(hd * hd + b * b);
-  T l2 = hm - r;
-  if (l2 >= eps) {
-    T det = a * c - b * b;
-    T di = T(1) / det;
-    inv[0] = c * di;
-    inv[1] = -b * di;
-    inv[2] = a * di;
-    return;
-  }
-  T l1 = hm + r;
-  T l1c = l1 > eps ? l1 : eps;
-  T l2c = eps;
-  if (r > T(0)) {
-    T r2 = r + r;
-    T pa = (a - l2) / r2, pb = b / r2, pc = (c - l2) / r2;
-    inv[0] = pa / l1c + (T(1) - pa) / l2c;
-    inv[1] = pb / l1c - pb / l2c;
-    inv[2] = pc / l1c + (T(1) - pc) / l2c;
-  } else {
-    inv[0] = T(1) / l2c;
-    inv[1] = T(0);
-    inv[2] = T(1) / l2c;
-  }
-}
-
-// Half extents of the ellipse x^T K x = 1, scaled by 3 (3-sigma box).
-template <class T>
-inline void conic_half_extent3(const T* k, T* hx, T* hy) {
-  T det = k[0] * k[2] - k[1] * k[1];
-  T ex = std::sqrt(k[2] / det);
-  T ey = std::sqrt(k[0] / det);
-  *hx = T(3) * ex;
-  *hy = T(3) * ey;
-}
+using namespace dsplat_geo;
 
 struct Proj {
   float px, py, ndcz;
@@ -214,85 +101,40 @@ inline uint32_t depth_bits(float ndcz) {
 }
 
 
-// Deterministic exp(x), identical operation for operation to the CUDA dexp():
-// Cody-Waite reduction x = n*ln2 + r (ln2 split into a high part with 9
-// trailing zero bits and a low part), degree-7 Taylor polynomial of e^r on
-// |r| <= ln2/2, exact 2^n scaling; results below 2^-126 flush to zero.  The
-// GPU blend and this oracle both use it so the 0.999 early-exit decisions are
-// reproducible bit for bit (libm expf and CUDA expf differ in the last ulp).
-inline float dexp_f32(float x) {
-  if (x != x) return x;
-  if (x < -87.0f) return 0.0f;
-  if (x > 88.5f) return INFINITY;
-  const float n = std::rint(x * 1.44269502162933349609375f);
-  float r = x - n * 0.693145751953125f;
-  r = r - n * 1.428606765330187045e-06f;
-  float p = 1.984126984126984e-04f;
-  p = p * r + 1.388888888888889e-03f;
-  p = p * r + 8.333333333333333e-03f;
-  p = p * r + 4.166666666666667e-02f;
-  p = p * r + 1.666666666666667e-01f;
-  p = p * r + 0.5f;
-  p = p * r + 1.0f;
-  p = p * r + 1.0f;
-  const int ni = int(n);
-  if (ni < -126) return 0.0f;
-  uint32_t bits = uint32_t(ni + 127) << 23;
-  float sc;
-  std::memcpy(&sc, &bits, 4);
-  return p * sc;
+// exp(x) correctly rounded to float: e^x evaluated in double and rounded
+// once.  glibc's double exp is accurate to well under one double ulp, and
+// (float)exp((double)x) equals (float)expl(x) for every float x checked in
+// [-110, 0], so this is the float nearest to e^x.  The CUDA kernels'
+// expf_cr is held to it bit for bit (tests/test_gpu_parity.py).
+inline float cr_expf(float x) { return float(std::exp(double(x))); }
+
+// The blend's arithmetic, del-splat-cpu's pnt2pixxyndcz.rs:86-93 (the same
+// expressions as splat_gauss.cu:96-106) in f32 with no contraction:
+//   q = A dx dx + B (dx dy + dy dx) + C dy dy   (mat2_sym::mult_vec_from_both_sides,
+//       left-to-right as written; the del-geo crate itself is absent)
+//   e = exp(-0.5 q) * opacity;  e_out = T e;  rgb += c * e_out (per channel);
+//   T *= 1 - e;  alpha_sum += e_out;  stop once alpha_sum > 0.999
+// Modes (bit flags):
+//   kBlendLibmExp  -- exp is the C library's expf (glibc), as in
+//                     del-splat-cpu's `f32::exp` and the CUDA kernel
+//                     compiled for the host; default: cr_expf.
+//   kBlendCudaStop -- the stop test of splat_gauss.cu:105, `alpha_sum >
+//                     0.999` compared in double (= alpha_sum >= 0.999f);
+//                     default: del-splat-cpu's f32 `alpha_sum > 0.999f`.
+constexpr int kBlendLibmExp = 1, kBlendCudaStop = 2;
+
+inline float quad_form(const float* m, float dx, float dy) {
+  const float d[2] = {dx, dy};
+  return mult_vec_from_both_sides(m, d, d);
 }
 
-// Deterministic 2^y, identical operation for operation to the CUDA
-// exp2_det(): y = n + f with n the nearest integer (adding 1.5 * 2^23 rounds
-// y where the float spacing is 1; n is read from the sum's bits), |f| <= 1/2,
-// the degree-5 minimax polynomial of 2^f (coefficients from fit_exp2.py) in
-// Horner form with fused multiply-adds (std::fma is exactly rounded, like
-// the GPU's fma), and exact scaling by 2^n through the exponent field.  Outside (-125, 123): 0 below,
-// +inf above, NaN stays NaN.
-inline float exp2_det_f32(float y) {
-  if (!(std::fabs(y + 1.f) < 124.f)) {
-    if (y != y) return y;
-    return y < 0.f ? 0.f : INFINITY;
-  }
-  const float t = y + 12582912.f;
-  const float f = y - (t - 12582912.f);
-  float p = 0.0013202981790527701f;
-  p = std::fma(p, f, 0.009674952365458012f);
-  p = std::fma(p, f, 0.055510472506284714f);
-  p = std::fma(p, f, 0.24022166430950165f);
-  p = std::fma(p, f, 0.6931465864181519f);
-  p = std::fma(p, f, 1.f);
-  uint32_t tb, pb, magic;
-  const float m = 12582912.f;
-  std::memcpy(&tb, &t, 4);
-  std::memcpy(&pb, &p, 4);
-  std::memcpy(&magic, &m, 4);
-  const uint32_t r = pb + ((tb - magic) << 23);
-  float out;
-  std::memcpy(&out, &r, 4);
-  return out;
+inline float blend_exp(float x, int mode) {
+  return (mode & kBlendLibmExp) ? ::expf(x) : cr_expf(x);
 }
 
-// exp(-q/2) * opacity for the blend, as the CUDA rasterisers evaluate it:
-// the conic is pre-scaled by k = -log2(e)/2 (kA, k2B, kC), then
-// y = (kA dx) dx + (k2B dx + kC dy) dy with two fused multiply-adds and
-// alpha = 2^y * opacity.  splat_gauss.cu:96-98 computes the same quantity as
-// exp(-0.5 * (A dx dx + B (dx dy + dy dx) + C dy dy)) * opacity; the two
-// differ only in rounding.
-constexpr float kNegHalfLog2e = -0.72134752044448170368f;
-inline float blend_alpha(const float* conic, float opacity, float dx, float dy) {
-  const float ka = conic[0] * kNegHalfLog2e;
-  const float kb2 = (conic[1] + conic[1]) * kNegHalfLog2e;
-  const float kc = conic[2] * kNegHalfLog2e;
-  const float kadxdx = (ka * dx) * dx, kb2dx = kb2 * dx;
-  const float y = std::fma(std::fma(kc, dy, kb2dx), dy, kadxdx);
-  return exp2_det_f32(y) * opacity;
+inline bool blend_stop(float alpha_sum, int mode) {
+  return (mode & kBlendCudaStop) ? (double(alpha_sum) > 0.999) : (alpha_sum > 0.999f);
 }
-
-// splat_gauss.cu:105: `alpha_sum > 0.999` compares in double; for a float
-// alpha_sum that is exactly `alpha_sum >= 0.999f` (0.999f > 0.999).
-constexpr float kAlphaBreak = 0.999f;
 
 inline bool in_aabb(const float* a, float x, float y) {
   return a[0] <= x && x <= a[2] && a[1] <= y && y <= a[3];
@@ -406,9 +248,10 @@ inline void eval_color(int sh_deg, const T* mean, const T* campos,
 
 }  // namespace
 
-// The deterministic 2^y of the blend, elementwise (accuracy tests).
-extern "C" void orc_exp2_det(int64_t n, const float* y, float* out) {
-  for (int64_t i = 0; i < n; ++i) out[i] = exp2_det_f32(y[i]);
+// cr_expf elementwise (checks of the CUDA expf_cr); threaded.
+extern "C" void orc_expf_cr(int64_t n, const float* x, float* out) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) out[i] = cr_expf(x[i]);
 }
 
 // ============================================================================
@@ -441,24 +284,9 @@ extern "C" void orc_circle_project(int64_t n, const float* xyz,
     float r1 = (1.f - q[1]) * 0.5f * float(h);
     float J[9];
     jacobian_transform(mvp, p, J);
-    // 3x3 inverse via the adjugate (column-major in and out)
-    float a = J[0], d = J[1], g = J[2], b = J[3], e = J[4], hh = J[5],
-          c = J[6], f = J[7], k = J[8];
-    float co0 = e * k - f * hh, co1 = f * g - d * k, co2 = d * hh - e * g;
-    float det = a * co0 + b * co1 + c * co2;
-    float inv_det = 1.f / det;
     float inv[9];
-    inv[0] = co0 * inv_det;
-    inv[1] = co1 * inv_det;
-    inv[2] = co2 * inv_det;
-    inv[3] = (c * hh - b * k) * inv_det;
-    inv[4] = (a * k - c * g) * inv_det;
-    inv[5] = (b * g - a * hh) * inv_det;
-    inv[6] = (b * f - c * e) * inv_det;
-    inv[7] = (c * d - a * f) * inv_det;
-    inv[8] = (a * e - b * d) * inv_det;
-    float nx = std::sqrt(inv[0] * inv[0] + inv[1] * inv[1] + inv[2] * inv[2]);
-    float ny = std::sqrt(inv[3] * inv[3] + inv[4] * inv[4] + inv[5] * inv[5]);
+    mat3_inverse(J, inv);
+    float nx = norm3(inv), ny = norm3(inv + 3);
     float rx = (1.f / nx) * 0.5f * float(w) * radius;
     float ry = (1.f / ny) * 0.5f * float(h) * radius;
     xyd[3 * i + 0] = r0;
@@ -539,7 +367,7 @@ inline int32_t blend_pixel(int ix, int iy, uint32_t start, uint32_t end,
                            const uint32_t* idx2pnt, const float* xyd,
                            const float* conic, const float* aabb,
                            const float* opacity, const float* rgb, float* out,
-                           float* outT) {
+                           float* outT, int mode) {
   const float tx = float(ix) + 0.5f, ty = float(iy) + 0.5f;
   float asum = 0.f, occ = 1.f;
   float c0 = out[0], c1 = out[1], c2 = out[2];
@@ -548,14 +376,14 @@ inline int32_t blend_pixel(int ix, int iy, uint32_t start, uint32_t end,
     const uint32_t g = idx2pnt[pos];
     if (!in_aabb(aabb + 4 * g, tx, ty)) continue;
     const float dx = tx - xyd[3 * g], dy = ty - xyd[3 * g + 1];
-    const float e = blend_alpha(conic + 3 * g, opacity[g], dx, dy);
+    const float e = blend_exp(-0.5f * quad_form(conic + 3 * g, dx, dy), mode) * opacity[g];
     const float eo = occ * e;
-    c0 = std::fma(rgb[3 * g + 0], eo, c0);
-    c1 = std::fma(rgb[3 * g + 1], eo, c1);
-    c2 = std::fma(rgb[3 * g + 2], eo, c2);
-    occ = occ - eo;
+    c0 += rgb[3 * g + 0] * eo;
+    c1 += rgb[3 * g + 1] * eo;
+    c2 += rgb[3 * g + 2] * eo;
+    occ *= 1.f - e;
     asum += eo;
-    if (asum >= kAlphaBreak) {
+    if (blend_stop(asum, mode)) {
       last = int32_t(pos);
       break;
     }
@@ -568,13 +396,12 @@ inline int32_t blend_pixel(int ix, int iy, uint32_t start, uint32_t end,
 }
 }  // namespace
 
-extern "C" void orc_gauss_rasterize_tiled(
+extern "C" void orc_gauss_rasterize_tiled_mode(
     int w, int h, int ts, const uint32_t* tile2idx, const uint32_t* idx2pnt,
     const float* xyd, const float* conic, const float* aabb,
     const float* opacity, const float* rgb, float* pix_rgb, float* pix_T,
-    int32_t* pix_last, int nthreads) {
+    int32_t* pix_last, int nthreads, int mode) {
   const int tw = (w + ts - 1) / ts;
-  (void)nthreads;
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1) collapse(2)
   for (int iy = 0; iy < h; ++iy)
     for (int ix = 0; ix < w; ++ix) {
@@ -583,22 +410,33 @@ extern "C" void orc_gauss_rasterize_tiled(
       float T;
       int32_t last = blend_pixel(ix, iy, tile2idx[t], tile2idx[t + 1], idx2pnt,
                                  xyd, conic, aabb, opacity, rgb,
-                                 pix_rgb + 3 * pix, &T);
+                                 pix_rgb + 3 * pix, &T, mode);
       if (pix_T) pix_T[pix] = T;
       if (pix_last) pix_last[pix] = last;
     }
 }
 
+extern "C" void orc_gauss_rasterize_tiled(
+    int w, int h, int ts, const uint32_t* tile2idx, const uint32_t* idx2pnt,
+    const float* xyd, const float* conic, const float* aabb,
+    const float* opacity, const float* rgb, float* pix_rgb, float* pix_T,
+    int32_t* pix_last, int nthreads) {
+  orc_gauss_rasterize_tiled_mode(w, h, ts, tile2idx, idx2pnt, xyd, conic, aabb,
+                                 opacity, rgb, pix_rgb, pix_T, pix_last,
+                                 nthreads, 0);
+}
+
 // pnt2pixxyndcz.rs:42-100: global stable sort by ndc_z+1, clip |ndc_z| >= 1.
-extern "C" void orc_gauss_render_naive(int64_t n, const float* xyd,
-                                       const float* conic, const float* aabb,
-                                       const float* opacity, const float* rgb,
-                                       int w, int h, float* pix_rgb) {
+extern "C" void orc_gauss_render_naive_mode(int64_t n, const float* xyd,
+                                            const float* conic, const float* aabb,
+                                            const float* opacity, const float* rgb,
+                                            int w, int h, float* pix_rgb, int mode) {
   std::vector<uint32_t> ord(n);
   std::iota(ord.begin(), ord.end(), 0u);
   std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
     return xyd[3 * a + 2] + 1.f < xyd[3 * b + 2] + 1.f;
   });
+#pragma omp parallel for schedule(dynamic, 4)
   for (int iy = 0; iy < h; ++iy)
     for (int ix = 0; ix < w; ++ix) {
       const float tx = float(ix) + 0.5f, ty = float(iy) + 0.5f;
@@ -610,16 +448,23 @@ extern "C" void orc_gauss_render_naive(int64_t n, const float* xyd,
         if (z <= -1.f || z >= 1.f) continue;
         if (!in_aabb(aabb + 4 * g, tx, ty)) continue;
         const float dx = tx - xyd[3 * g], dy = ty - xyd[3 * g + 1];
-        const float e = blend_alpha(conic + 3 * g, opacity[g], dx, dy);
+        const float e = blend_exp(-0.5f * quad_form(conic + 3 * g, dx, dy), mode) * opacity[g];
         const float eo = occ * e;
-        o[0] = std::fma(rgb[3 * g + 0], eo, o[0]);
-        o[1] = std::fma(rgb[3 * g + 1], eo, o[1]);
-        o[2] = std::fma(rgb[3 * g + 2], eo, o[2]);
-        occ = occ - eo;
+        o[0] += rgb[3 * g + 0] * eo;
+        o[1] += rgb[3 * g + 1] * eo;
+        o[2] += rgb[3 * g + 2] * eo;
+        occ *= 1.f - e;
         asum += eo;
-        if (asum >= kAlphaBreak) break;
+        if (blend_stop(asum, mode)) break;
       }
     }
+}
+
+extern "C" void orc_gauss_render_naive(int64_t n, const float* xyd,
+                                       const float* conic, const float* aabb,
+                                       const float* opacity, const float* rgb,
+                                       int w, int h, float* pix_rgb) {
+  orc_gauss_render_naive_mode(n, xyd, conic, aabb, opacity, rgb, w, h, pix_rgb, 0);
 }
 
 // splat_circle.cu:93-132: ascending walk, the last covering entry wins.
@@ -698,8 +543,8 @@ extern "C" void orc_fused_project(int64_t n, const float* means,
                                   float* rgb) {
   const int K = sh_count(sh_deg);
   for (int64_t i = 0; i < n; ++i) {
-    float s[3] = {dexp_f32(log_scales[3 * i]), dexp_f32(log_scales[3 * i + 1]),
-                  dexp_f32(log_scales[3 * i + 2])};
+    float s[3] = {cr_expf(log_scales[3 * i]), cr_expf(log_scales[3 * i + 1]),
+                  cr_expf(log_scales[3 * i + 2])};
     float qn[4];
     normalize_quat(quats + 4 * i, qn);
     Proj p;

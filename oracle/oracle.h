@@ -6,11 +6,14 @@
  * and bench.py's CPU-baseline / reference arms may load it.  Nothing in the
  * product path calls it.
  *
- * Parity status (see DESIGN.md "Oracle"): the tile-pair key format, the tile
- * span and the point z-buffer are pinned against the reference's own CUDA
+ * Parity status: the tile-pair key format, the tile span, the point
+ * z-buffer and the blend (splat_gauss.cu:56-109, with the C library's expf
+ * and its double stop test) are pinned against the reference's own CUDA
  * sources compiled on the CPU (oracle/ref/, output oracle/_ref/).  The
- * projection maths lives in the absent del-geo crate and is restated here;
- * that part is "parity unpinned" (no golden vector exists upstream).
+ * del-geo helpers those sources call (matrix products, the projected
+ * covariance, its safe inverse, the quadratic form) live in an absent crate
+ * and are restated here; that part is "parity unpinned" (no golden vector
+ * exists upstream).
  *
  * Conventions (all arrays row-major, f32 unless stated):
  *   mvp[16]            column-major 4x4 world->NDC, larger ndc_z = nearer
@@ -40,15 +43,32 @@ uint64_t orc_tile2pnt_count(int64_t n, const float* aabb, int tile_w,
 void orc_tile2pnt_fill(int64_t n, const float* aabb, const float* xyd,
                        int tile_w, int tile_h, int ts, const uint32_t* tile2idx,
                        uint32_t* idx2pnt, uint64_t* keys);
+/* Blend (pnt2pixxyndcz.rs:86-93 arithmetic).  mode bit 1: the C library's
+ * expf instead of the correctly rounded exp; mode bit 2: the CUDA kernel's
+ * double stop test (alpha_sum >= 0.999f) instead of del-splat-cpu's
+ * alpha_sum > 0.999f.  The plain entry points use mode 0. */
 void orc_gauss_rasterize_tiled(int w, int h, int ts, const uint32_t* tile2idx,
                                const uint32_t* idx2pnt, const float* xyd,
                                const float* conic, const float* aabb,
                                const float* opacity, const float* rgb,
                                float* pix_rgb, float* pix_T,
                                int32_t* pix_last, int nthreads);
+void orc_gauss_rasterize_tiled_mode(int w, int h, int ts,
+                                    const uint32_t* tile2idx,
+                                    const uint32_t* idx2pnt, const float* xyd,
+                                    const float* conic, const float* aabb,
+                                    const float* opacity, const float* rgb,
+                                    float* pix_rgb, float* pix_T,
+                                    int32_t* pix_last, int nthreads, int mode);
 void orc_gauss_render_naive(int64_t n, const float* xyd, const float* conic,
                             const float* aabb, const float* opacity,
                             const float* rgb, int w, int h, float* pix_rgb);
+void orc_gauss_render_naive_mode(int64_t n, const float* xyd,
+                                 const float* conic, const float* aabb,
+                                 const float* opacity, const float* rgb, int w,
+                                 int h, float* pix_rgb, int mode);
+/* exp(x) correctly rounded to float, elementwise */
+void orc_expf_cr(int64_t n, const float* x, float* out);
 void orc_circle_splat_tiled(int w, int h, int ts, const uint32_t* tile2idx,
                             const uint32_t* idx2pnt, const float* xyd,
                             const float* rad, int32_t* winner);

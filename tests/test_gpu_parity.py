@@ -1,0 +1,134 @@
+"""The blend against the reference's own arithmetic (
+images and alpha within max-abs 1e-4 of del-splat-cpu's FP32 blend).
+
+Three comparators, all on the CPU:
+  * the oracle's mode 0 -- the product's specification: del-splat-cpu's f32
+    operations (pnt2pixxyndcz.rs:86-93) with a correctly rounded exp; the GPU
+    must equal it bit for bit;
+  * the oracle with BLEND_LIBM_EXP -- del-splat-cpu literally (glibc expf,
+    f32 stop test): max-abs <= 1e-4 on images and alpha, and the fraction of
+    pixels whose stop position differs is printed;
+  * the reference's splat_gauss.cu compiled for the host (oracle/_ref) -- the
+    reference CUDA kernel's arithmetic with its double stop test, compared
+    with the GPU run under DSPLAT_STOP_CUDA.
+And the GPU's exp itself on every float."""
+import numpy as np
+import pytest
+import torch
+
+from dsplat import _native as N
+from dsplat import cudarc, scenes
+from dsplat.gauss import GaussBatch
+from gpu_util import F, T, U32, params_of
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def test_expf_cr_on_every_float(orc, dev):
+    """dsplat_expf_cr == the correctly rounded e^x for all 2^32 inputs (NaN
+    inputs: NaN out)."""
+    chunk = 1 << 26
+    bad = 0
+    for c in range((1 << 32) // chunk):
+        x = np.arange(c * chunk, (c + 1) * chunk, dtype=np.uint64).astype(np.uint32).view(np.float32)
+        y = F(cudarc.expf_cr(T(x, dev)))
+        want = orc.expf_cr(x)
+        same = y.view(np.uint32) == want.view(np.uint32)
+        same |= np.isnan(y) & np.isnan(want)
+        bad += int((~same).sum())
+    assert bad == 0
+
+
+def _dropin(dev, sc, size, ts, stop_rule=N.STOP_CPU):
+    cam = sc.cameras[0]
+    n = sc.n
+    xyd, conic, aabb = (torch.empty((n, k), device=dev) for k in (3, 3, 4))
+    cudarc.splat_gauss_pnt2splat3_to_pnt2splat2(None, T(sc.means, dev), T(sc.scales, dev), T(sc.quats, dev), xyd,
+                                                conic, aabb, T(cam.mvp, dev), size)
+    t2i, i2p = cudarc.splat_gauss_tile2idx_idx2pnt(None, size, ts, xyd, aabb)
+    w, h = size
+    img = torch.zeros((h, w, 3), device=dev)
+    Tm = torch.empty((h, w), device=dev)
+    stop = torch.empty((h, w), dtype=torch.int32, device=dev)
+    cudarc.splat_gauss_rasterize_pnt2splat2(None, size, img, xyd, conic, aabb, T(sc.opacity, dev), T(sc.colors, dev),
+                                            ts, t2i, i2p, Tm, stop, stop_rule=stop_rule)
+    torch.cuda.synchronize()
+    return dict(img=F(img), T=F(Tm), stop=F(stop), xyd=F(xyd), conic=F(conic), aabb=F(aabb), t2i=U32(t2i),
+                i2p=U32(i2p))
+
+
+def _report(tag, img, Tm, stop, o_img, o_T, o_stop):
+    d_img = float(np.abs(img - o_img).max())
+    d_alpha = float(np.abs((1 - Tm) - (1 - o_T)).max())
+    moved = float((stop != o_stop).mean())
+    print(f"{tag}: max|img| {d_img:.3g}, max|alpha| {d_alpha:.3g}, stop position differs on {moved:.2e} of pixels")
+    return d_img, d_alpha
+
+
+@pytest.mark.parametrize("ts", [16, 8, 32])
+def test_config0_dropin_against_del_splat_cpu(orc, dev, ts):
+    """16,384 Gaussians, 256x256 (config 0) through the drop-in chain."""
+    size = (256, 256)
+    sc = scenes.config0(n=16384, size=size)
+    g = _dropin(dev, sc, size, ts)
+    args = (256, 256, ts, g["t2i"], g["i2p"], g["xyd"], g["conic"], g["aabb"], sc.opacity, sc.colors)
+    o_img, o_T, o_stop = orc.gauss_rasterize_tiled(*args, nthreads=8)
+    assert np.array_equal(g["img"].view(np.uint32), o_img.view(np.uint32))
+    assert np.array_equal(g["T"].view(np.uint32), o_T.view(np.uint32))
+    assert np.array_equal(g["stop"], o_stop)
+    c_img, c_T, c_stop = orc.gauss_rasterize_tiled(*args, nthreads=8, mode=orc.BLEND_LIBM_EXP)
+    d_img, d_alpha = _report(f"config0 ts{ts} vs del-splat-cpu", g["img"], g["T"], g["stop"], c_img, c_T, c_stop)
+    assert d_img <= TOL and d_alpha <= TOL
+    # del-splat-cpu's own untiled renderer (global depth sort) as well
+    naive = orc.gauss_render_naive(g["xyd"], g["conic"], g["aabb"], sc.opacity, sc.colors, 256, 256,
+                                   mode=orc.BLEND_LIBM_EXP)
+    assert float(np.abs(g["img"] - naive).max()) <= TOL
+
+
+def test_config0_cuda_stop_rule_against_reference_kernel(orc, dev):
+    """DSPLAT_STOP_CUDA against the reference CUDA kernel's own source run on
+    the host (C library expf, `alpha_sum > 0.999` in double)."""
+    if not orc.ref_available():
+        pytest.skip("oracle/_ref not built")
+    size, ts = (256, 256), 16
+    sc = scenes.config0(n=16384, size=size)
+    g = _dropin(dev, sc, size, ts, stop_rule=N.STOP_CUDA)
+    args = (256, 256, ts, g["t2i"], g["i2p"], g["xyd"], g["conic"], g["aabb"], sc.opacity, sc.colors)
+    o_img, o_T, o_stop = orc.gauss_rasterize_tiled(*args, nthreads=8, mode=orc.BLEND_CUDA_STOP)
+    assert np.array_equal(g["img"].view(np.uint32), o_img.view(np.uint32))
+    assert np.array_equal(g["stop"], o_stop)
+    ref = orc.ref_gauss_rasterize(*args)
+    d = float(np.abs(g["img"] - ref).max())
+    print(f"config0 STOP_CUDA vs splat_gauss.cu on the host: max|img| {d:.3g}")
+    assert d <= TOL
+
+
+def test_1080p_sh3_view_against_del_splat_cpu(orc, dev):
+    """One 1920x1080 view of the 1,048,576-Gaussian SH-3 scene (config 3)
+    through the batched path, against del-splat-cpu's blend on the oracle's
+    projection and tile lists."""
+    sc = scenes.config3(n=1 << 20, views=16)
+    cam = next(c for c in sc.cameras if c.width == 1920)
+    sc.cameras = [cam]
+    batch = GaussBatch(sc.n, [cam], 8, 3, device=dev)
+    p = params_of(sc, dev)
+    batch.ensure_capacity(p)
+    batch.forward(p)
+    torch.cuda.synchronize()
+    img = F(batch.images()[0])
+    Tm = F(batch.per_pixel("T")[0])
+    xyd, conic, aabb, rgb = orc.fused_project(sc.means, sc.log_scales, sc.quats, sc.colors, 3, cam.mvp, cam.campos,
+                                              1920, 1080)
+    t2i, i2p, _ = orc.tile2pnt(xyd, aabb, 1920, 1080, 16, with_keys=False)
+    args = (1920, 1080, 16, t2i, i2p, xyd, conic, aabb, sc.opacity, rgb)
+    o_img, o_T, o_stop = orc.gauss_rasterize_tiled(*args, nthreads=16)
+    assert np.array_equal(img.view(np.uint32), o_img.view(np.uint32))
+    assert np.array_equal(Tm.view(np.uint32), o_T.view(np.uint32))
+    c_img, c_T, c_stop = orc.gauss_rasterize_tiled(*args, nthreads=16, mode=orc.BLEND_LIBM_EXP)
+    d_img = float(np.abs(img - c_img).max())
+    d_alpha = float(np.abs(Tm - c_T).max())
+    moved = float((o_stop != c_stop).mean())
+    print(f"1080p SH3 vs del-splat-cpu: max|img| {d_img:.3g}, max|alpha| {d_alpha:.3g}, "
+          f"stop position differs on {moved:.2e} of pixels")
+    assert d_img <= TOL and d_alpha <= TOL
