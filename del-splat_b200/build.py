@@ -5,8 +5,10 @@
 Every .cu under csrc/ is compiled with nvcc for sm_100a only and linked into
 one shared library with the CUDA runtime linked statically, so the library
 does not depend on the libcudart that the host process (e.g. torch) loaded.
-project.cu is compiled with -fmad=false: its FP32 results must match the CPU
-oracle bit for bit (tile spans and sort keys derive from them).
+project.cu and raster_fwd.cu are compiled with -fmad=false: their FP32
+results must match the CPU oracle bit for bit (tile spans and sort keys derive
+from the projection; the blend follows del-splat-cpu's operations), so no
+multiply-add may be fused that the source does not write as an fma.
 """
 from __future__ import annotations
 
@@ -28,7 +30,7 @@ LIB = os.path.join(OUT_DIR, "libdsplat.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC,
           "--expt-relaxed-constexpr", "-Xptxas", "-v"]
-PER_FILE = {"project.cu": ["-fmad=false"]}
+PER_FILE = {"project.cu": ["-fmad=false"], "raster_fwd.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

@@ -29,7 +29,8 @@ __global__ void k_pair_cost(const ViewBatch, int, const uint32_t*, uint32_t*);
 int raster_bwd_group(int ts);
 int raster_fwd_group(int ts);
 __global__ void k_iota_pad(uint32_t*, uint32_t*, uint32_t, uint32_t, uint32_t);
-__global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*, uint32_t*);
+__global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*,
+                           unsigned long long*);
 __global__ void k_sb_scatter(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
                              uint64_t, uint2*, uint32_t*);
 __global__ void k_sb_scatter_staged(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
@@ -39,8 +40,9 @@ __global__ void k_tile_count(const uint2*, const uint32_t*, uint32_t, uint64_t, 
 __global__ void k_tile_scatter(const uint2*, const uint32_t*, uint32_t, uint64_t, const ViewBatch, const uint32_t*,
                                uint32_t*, uint32_t*, uint32_t*);
 __global__ void k_clamp_ranges(uint32_t*, uint32_t, uint64_t, uint32_t*);
-__global__ void k_copy_total(const uint32_t*, size_t, uint32_t*);
-__global__ void k_make_keys64(const uint32_t*, const uint32_t*, const float*, const uint32_t*, uint64_t, uint64_t*);
+__global__ void k_check_capacity(const unsigned long long*, uint64_t, uint32_t*);
+__global__ void k_make_keys64(const uint32_t*, const uint32_t*, const float*, const unsigned long long*, uint64_t,
+                              uint64_t*);
 __global__ void k_fill_u64(uint64_t*, size_t, uint64_t);
 __global__ void k_point_zbuf(uint32_t, const float*, int, int, uint64_t*);
 __global__ void k_point_resolve(size_t, const uint64_t*, const float*, const float*, float*, float*, int32_t*);
@@ -65,6 +67,9 @@ cudaError_t raster_fwd_aos(cudaStream_t, int, int, int, float*, const float*, co
 cudaError_t expf_cr_launch(cudaStream_t, size_t, const float*, float*);
 cudaError_t circle_splat_tiles(cudaStream_t, int, int, int, float*, const float*, const float*, const float*,
                                const uint32_t*, const uint32_t*);
+
+__global__ void k_adam_fused(AdamSeg, float, float, float, float, const int32_t*);
+__global__ void k_adam_step_inc(int32_t*);
 
 __global__ void k_one_minus(const float* __restrict__ T, float* __restrict__ out, size_t n) {
   const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -153,7 +158,8 @@ void carve_lists(Carver& c, const ViewBatch& b, uint32_t npad, size_t cap, Lists
 }
 
 // Stage 1: superblock lists of (point, local tile span) in rank order.
-// flags[1] <- tile pairs P, flags[4] <- superblock entries (capacity needed).
+// flags[6..7] <- tile pairs P (u64), flags[8..9] <- superblock entries
+// (capacity needed, u64); flags[0] |= overflow when they exceed capacity.
 int build_sb_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npad, const uint32_t* order,
                    const uint2* srect, const ListsWs& L, uint32_t* scan_tmp, uint64_t capacity, uint32_t* flags) {
   const uint32_t nchunk = npad / kChunk;
@@ -165,11 +171,12 @@ int build_sb_lists(cudaStream_t st, const ViewBatch& b, uint32_t n, uint32_t npa
     if (smem3 > 200 * 1024) return fail(DSPLAT_ERR_UNSUPPORTED, "too many superblocks in one view");
     TRY_CUDA(cudaFuncSetAttribute(k_sb_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)), "attr");
   }
-  k_sb_count<<<grid1, 256, smem1, st>>>(order, srect, n, npad, b, L.cnt1, flags + 1);
+  unsigned long long* totals = reinterpret_cast<unsigned long long*>(flags + 6);
+  k_sb_count<<<grid1, 256, smem1, st>>>(order, srect, n, npad, b, L.cnt1, totals);
   count_launch();
   TRY_CUDA(cudaMemsetAsync(L.cnt1 + m, 0, sizeof(uint32_t), st), "memset");
   TRY_CUDA(exclusive_scan(st, L.cnt1, L.off1, m + 1, scan_tmp), "scan");
-  k_copy_total<<<1, 32, 0, st>>>(L.off1, m, flags + 4);
+  k_check_capacity<<<1, 32, 0, st>>>(totals + 1, capacity, flags);
   count_launch();
   // staged scatter (coalesced list stores) when its shared memory fits
   constexpr uint32_t kStageEntries = 3072;
@@ -371,7 +378,8 @@ int tiles_fill(cudaStream_t st, uint32_t n, const float* xyd, const float* aabb,
                         t.flags);
   if (rc) return rc;
   if (keys64) {
-    k_make_keys64<<<1184, 256, 0, st>>>(t.out_tile, idx2pnt, xyd, t.flags + 1, capacity, keys64);
+    k_make_keys64<<<1184, 256, 0, st>>>(t.out_tile, idx2pnt, xyd,
+                                        reinterpret_cast<const unsigned long long*>(t.flags + 6), capacity, keys64);
     count_launch();
   }
   TRY_CUDA(cudaGetLastError(), "launch");
@@ -814,14 +822,53 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
 int dsplat_gauss_batch_status(dsplat_stream stream, const void* workspace, uint32_t* flags, uint64_t* capacity_needed,
                               uint64_t* tile_pairs) {
   if (!workspace) return fail(DSPLAT_ERR_INVALID_ARG, "workspace is null");
-  uint32_t h[5] = {0, 0, 0, 0, 0};
+  uint32_t h[10] = {};
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   TRY_CUDA(cudaMemcpyAsync(h, workspace, sizeof(h), cudaMemcpyDeviceToHost, st), "memcpy");
   TRY_CUDA(cudaStreamSynchronize(st), "sync");
+  uint64_t pairs, entries;
+  memcpy(&pairs, h + 6, 8);
+  memcpy(&entries, h + 8, 8);
   if (flags) *flags = h[0];
-  if (capacity_needed) *capacity_needed = h[4];
-  if (tile_pairs) *tile_pairs = h[1];
+  if (capacity_needed) *capacity_needed = entries;
+  if (tile_pairs) *tile_pairs = pairs;
   return (h[0] & kFlagPairOverflow) ? DSPLAT_ERR_CAPACITY : DSPLAT_OK;
+}
+
+int dsplat_gauss_adam_step(dsplat_stream stream, int64_t num_pnt, int32_t sh_degree,
+                           const dsplat_gauss_tensors* params, const dsplat_gauss_grads* grads,
+                           const dsplat_gauss_tensors* exp_avg, const dsplat_gauss_tensors* exp_avg_sq, float lr,
+                           float beta1, float beta2, float eps, int32_t* step) {
+  if (num_pnt <= 0) return DSPLAT_OK;
+  if (!params || !grads || !exp_avg || !exp_avg_sq || !step) return fail(DSPLAT_ERR_INVALID_ARG, "null argument");
+  if (sh_degree < -1 || sh_degree > 3) return fail(DSPLAT_ERR_INVALID_ARG, "sh_degree must be -1..3");
+  const size_t n = size_t(num_pnt);
+  const size_t K = sh_degree < 0 ? 1 : size_t(sh_degree + 1) * size_t(sh_degree + 1);
+  const size_t counts[5] = {3 * n, 3 * n, 4 * n, n, 3 * K * n};
+  float* const ps[5] = {params->means, params->log_scales, params->quats, params->opacity, params->colors};
+  const float* const gs[5] = {grads->means, grads->log_scales, grads->quats, grads->opacity, grads->colors};
+  float* const ms[5] = {exp_avg->means, exp_avg->log_scales, exp_avg->quats, exp_avg->opacity, exp_avg->colors};
+  float* const vs[5] = {exp_avg_sq->means, exp_avg_sq->log_scales, exp_avg_sq->quats, exp_avg_sq->opacity,
+                        exp_avg_sq->colors};
+  AdamSeg seg;
+  size_t acc = 0;
+  for (int k = 0; k < 5; ++k) {
+    if (!ps[k] || !gs[k] || !ms[k] || !vs[k]) return fail(DSPLAT_ERR_INVALID_ARG, "null tensor");
+    seg.p[k] = ps[k];
+    seg.g[k] = gs[k];
+    seg.m[k] = ms[k];
+    seg.v[k] = vs[k];
+    acc += counts[k];
+    seg.end[k] = acc;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_adam_fused<<<unsigned(std::min<size_t>(blocks_for(acc, 256), 148 * 16)), 256, 0, st>>>(seg, lr, beta1, beta2,
+                                                                                         eps, step);
+  count_launch();
+  k_adam_step_inc<<<1, 32, 0, st>>>(step);
+  count_launch();
+  TRY_CUDA(cudaGetLastError(), "adam");
+  return DSPLAT_OK;
 }
 
 int dsplat_adam_step(dsplat_stream stream, int64_t n, float* param, const float* grad, float* exp_avg,

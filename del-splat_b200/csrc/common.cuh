@@ -86,6 +86,15 @@ struct BwdArgs {
 
 
 
+// The five parameter tensors of one fused Adam launch (k_adam_fused).
+struct AdamSeg {
+  float* p[5];
+  const float* g[5];
+  float* m[5];
+  float* v[5];
+  size_t end[5];  // cumulative element counts
+};
+
 __device__ __forceinline__ int view_of_item(const ViewBatch& b, uint32_t item) {
   int v = 0;
 #pragma unroll 1
@@ -149,6 +158,15 @@ __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
 }
 
 __device__ __forceinline__ f2 neg2(f2 a) { return a ^ 0x8000000080000000ull; }
+
+// A packed product that keeps its own rounding when it feeds an add.  The
+// assembler fuses a mul.rn.f32x2 whose result goes into an add.rn.f32x2 into
+// one fused multiply-add (a single rounding) -- with or without -fmad=false,
+// unlike the scalar mul.rn/add.rn pairs -- which changes the sum by an ulp
+// now and then.  fma(a, b, -0) equals RN(a b) exactly (signed zeros
+// included), and with the -0 held in a runtime value (nz: a kernel argument,
+// (-0, -0)) there is no product left to fuse.
+__device__ __forceinline__ f2 mul2_rn(f2 a, f2 b, f2 nz) { return fma2(a, b, nz); }
 
 // ---------------------------------------------------------------------------
 // expf_cr: e^x correctly rounded to single precision (the float nearest to
@@ -239,9 +257,10 @@ __device__ __forceinline__ float expf_cr(float x) {
 
 // Packed form for two elements, table in shared memory (tab: a copy of
 // g_exp2_64).  RANGE: check |x| <= 87 per element (a caller that has bounded
-// x for a whole batch passes false).  Each element equals expf_cr of it.
+// x for a whole batch passes false).  nz: (-0, -0) held in a runtime value
+// (see mul2_rn).  Each element equals expf_cr of it.
 template <bool RANGE>
-__device__ __forceinline__ f2 expf_cr2(f2 x, const float2* tab) {
+__device__ __forceinline__ f2 expf_cr2(f2 x, const float2* tab, f2 nz) {
   const f2 tk = fma2(x, f2_dup(kExpK64), f2_dup(kExpMagic));
   const f2 kf = sub2(tk, f2_dup(kExpMagic));
   const f2 r1 = fma2(kf, f2_dup(-kExpC1), x);
@@ -255,7 +274,7 @@ __device__ __forceinline__ f2 expf_cr2(f2 x, const float2* tab) {
   const uint32_t b0 = __float_as_uint(f2_lo(tk)), b1 = __float_as_uint(f2_hi(tk));
   const float2 t0 = tab[b0 & 63u], t1 = tab[b1 & 63u];
   const f2 th = f2_make(t0.x, t1.x), tl = f2_make(t0.y, t1.y);
-  const f2 ph = mul2(th, rh), pl = fma2(th, rh, neg2(ph));
+  const f2 ph = mul2_rn(th, rh, nz), pl = fma2(th, rh, neg2(ph));
   const f2 s = add2(th, ph), e1 = sub2(ph, sub2(s, th));
   const f2 a = add2(fma2(th, tail, pl), e1);
   const f2 ylo = add2(a, fma2(tl, rh, tl));

@@ -382,4 +382,38 @@ __global__ void k_adam(size_t n, float* __restrict__ p, const float* __restrict_
   p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
 }
 
+// Fused Adam over the five parameter tensors of a Gaussian scene (one
+// launch), with the step count kept on the device so that a captured graph
+// replays correctly: every thread reads t = *step + 1 and k_adam_step_inc
+// stores it after the update.  Same update as torch.optim.Adam (no weight
+// decay, no amsgrad): m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2,
+// p -= lr (m / (1 - b1^t)) / (sqrt(v / (1 - b2^t)) + eps).  The opacity
+// tensor is then kept in [0, kOpacityMax]: the blend needs alpha < 1 (the
+// backward rebuilds T in front of an entry as T / (1 - alpha)).
+constexpr float kOpacityMax = 0.999f;
+
+__global__ void k_adam_fused(AdamSeg seg, float lr, float b1, float b2, float eps, const int32_t* __restrict__ step) {
+  const size_t total = seg.end[4];
+  const float t = float(*step + 1);
+  const float bc1 = 1.f - powf(b1, t), bc2 = 1.f - powf(b2, t);
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+    int k = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) k += i >= seg.end[j];
+    const size_t o = i - (k ? seg.end[k - 1] : 0);
+    const float gi = seg.g[k][o];
+    const float mi = b1 * seg.m[k][o] + (1.f - b1) * gi;
+    const float vi = b2 * seg.v[k][o] + (1.f - b2) * gi * gi;
+    seg.m[k][o] = mi;
+    seg.v[k][o] = vi;
+    float pi = seg.p[k][o] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    if (k == 3) pi = fminf(fmaxf(pi, 0.f), kOpacityMax);
+    seg.p[k][o] = pi;
+  }
+}
+
+__global__ void k_adam_step_inc(int32_t* step) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
+}
+
 }  // namespace dsplat

@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restr
                                                          const uint2* __restrict__ srect, uint32_t n, uint32_t npad,
                                                          const ViewBatch b,
                                                          uint32_t* __restrict__ cnt,
-                                                         uint32_t* __restrict__ total_pairs) {
+                                                         unsigned long long* __restrict__ totals) {
   extern __shared__ uint32_t hist[];
   const uint32_t nchunk = npad / kMsChunk;
   const uint32_t v = blockIdx.x / nchunk, c = blockIdx.x % nchunk;
@@ -356,19 +356,28 @@ __global__ void __launch_bounds__(kMsThreads) k_sb_count(const uint32_t* __restr
   for (int i = threadIdx.x; i < nsb; i += kMsThreads) hist[i] = 0;
   __syncthreads();
   const size_t base = size_t(v) * npad + size_t(c) * kMsChunk;
-  uint32_t pairs = 0;
+  unsigned long long pairs = 0, entries = 0;
   for (int i = threadIdx.x; i < kMsChunk; i += kMsThreads) {
     const uint2 rc = srect[base + i];
     int sx0, sy0, sx1, sy1;
     if (!sb_span(rc, sl, &sx0, &sy0, &sx1, &sy1)) continue;
-    pairs += uint32_t((rc.y & 0xffff) - (rc.x & 0xffff)) * uint32_t((rc.y >> 16) - (rc.x >> 16));
+    pairs += (unsigned long long)((rc.y & 0xffff) - (rc.x & 0xffff)) * ((rc.y >> 16) - (rc.x >> 16));
+    entries += (unsigned long long)(sx1 - sx0) * (sy1 - sy0);
     for (int sy = sy0; sy < sy1; ++sy)
       for (int sx = sx0; sx < sx1; ++sx) atomicAdd(&hist[sy * sbw + sx], 1u);
   }
-  // exact pair total (tile-span areas), known even when a later stage overflows
+  // exact 64-bit totals of tile pairs (tile-span areas) and superblock
+  // entries, known even when a later stage overflows or a 32-bit list offset
+  // wraps
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
-  if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(total_pairs, pairs);
+  for (int o = 16; o > 0; o >>= 1) {
+    pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+    entries += __shfl_xor_sync(0xffffffffu, entries, o);
+  }
+  if ((threadIdx.x & 31) == 0 && entries) {
+    atomicAdd(&totals[0], pairs);
+    atomicAdd(&totals[1], entries);
+  }
   __syncthreads();
   const uint32_t sb0 = vd.sb_base;
   for (int i = threadIdx.x; i < nsb; i += kMsThreads) cnt[(size_t(sb0) + i) * nchunk + c] = hist[i];
@@ -824,17 +833,19 @@ __global__ void k_clamp_ranges(uint32_t* __restrict__ item_start, uint32_t num_i
     if (item_start[i] > capacity) item_start[i] = uint32_t(capacity);
 }
 
-__global__ void k_copy_total(const uint32_t* __restrict__ off, size_t idx, uint32_t* __restrict__ out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) *out = off[idx];
+// Flags a capacity overflow when the superblock lists need more entries than
+// the capacity (the 64-bit total also catches a wrapped 32-bit offset scan).
+__global__ void k_check_capacity(const unsigned long long* __restrict__ entries, uint64_t capacity,
+                                 uint32_t* __restrict__ flags) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && *entries > capacity) set_flag(flags, kFlagPairOverflow);
 }
 
 // keys for the drop-in API: idx2tiledepth = (tile << 32) | depth bits of the
 // point, recomputed from pnt2pixxydepth
 __global__ void k_make_keys64(const uint32_t* __restrict__ tile, const uint32_t* __restrict__ pnt,
-                              const float* __restrict__ xyd, const uint32_t* __restrict__ count_ptr,
+                              const float* __restrict__ xyd, const unsigned long long* __restrict__ count_ptr,
                               uint64_t capacity, uint64_t* __restrict__ out) {
-  uint32_t cnt = *count_ptr;
-  if (cnt > capacity) cnt = uint32_t(capacity);
+  const uint64_t cnt = *count_ptr < capacity ? uint64_t(*count_ptr) : capacity;
   for (size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p < cnt; p += size_t(gridDim.x) * blockDim.x)
     out[p] = (uint64_t(tile[p]) << 32) | depth_bits(xyd[3 * size_t(pnt[p]) + 2]);
 }

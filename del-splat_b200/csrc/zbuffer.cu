@@ -21,7 +21,6 @@
 // 0xFFFFFFFE).
 #include <cfloat>
 #include <cstdio>
-#include <mutex>
 
 #include "common.cuh"
 
@@ -150,25 +149,20 @@ static __device__ __align__(256) unsigned long long g_noalloc_zbuf[kNoAllocMaxPi
 int report_error(int code, const char* msg);
 
 namespace {
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[kMaxDevices] = {};
-
 // Device address of g_noalloc_zbuf on the current device (host code only sees
-// a host-side stand-in under that name).  Looked up once per device.
+// a host-side stand-in under that name).  Looked up on every call, with the
+// caller's device current: the lookup is cheap, and a cached address would go
+// stale if the caller reset the device (the module, and the array with it,
+// is then loaded again at another address).
 int noalloc_scratch(uint64_t** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return report_error(DSPLAT_ERR_CUDA, "cudaGetDevice failed");
-  if (dev < 0 || dev >= kMaxDevices) return report_error(DSPLAT_ERR_UNSUPPORTED, "device index out of range");
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_zbuf);
-    if (e != cudaSuccess || !p) return report_error(DSPLAT_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_zbuf) failed");
-    g_noalloc_addr[dev] = p;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_zbuf);
+  if (e != cudaSuccess || !p) {
+    char msg[200];
+    snprintf(msg, sizeof(msg), "cudaGetSymbolAddress(g_noalloc_zbuf) failed: %s", cudaGetErrorString(e));
+    return report_error(DSPLAT_ERR_CUDA, msg);
   }
-  *out = static_cast<uint64_t*>(g_noalloc_addr[dev]);
+  *out = static_cast<uint64_t*>(p);
   return DSPLAT_OK;
 }
 }  // namespace
@@ -176,9 +170,10 @@ int noalloc_scratch(uint64_t** out) {
 
 // Same contract and results as dsplat_point_rasterize_pix_zbuffer, without the
 // zbuf argument: the keys are kept in the library's own 2^20-entry device
-// array.  Images larger than 2^20 pixels are rejected.  The first call on a
-// device looks the array up (cudaGetSymbolAddress) -- make that first call
-// before any stream capture.  All calls share the one array (it is refilled at
+// array.  Images larger than 2^20 pixels are rejected.  Every call looks the
+// array's device address up (cudaGetSymbolAddress) on the current device; the
+// first call on a device also loads the library's module there -- make that
+// first call before any stream capture.  All calls share the one array (it is refilled at
 // the start of every call), so calls whose GPU work overlaps -- on different
 // streams or host threads -- race and must be serialised by the caller.
 extern "C" int dsplat_point_rasterize_pix_zbuffer_noalloc(dsplat_stream stream, uint32_t num_pnt,

@@ -50,6 +50,11 @@ class GaussGrads(ctypes.Structure):
                 ("colors", c_void_p)]
 
 
+class GaussTensors(ctypes.Structure):
+    _fields_ = [("means", c_void_p), ("log_scales", c_void_p), ("quats", c_void_p), ("opacity", c_void_p),
+                ("colors", c_void_p)]
+
+
 class BatchLayout(ctypes.Structure):
     _fields_ = [("total_bytes", c_size), ("num_items", c_u32), ("num_pix", c_u32), ("npad", c_u32),
                 ("slabs_per_tile", c_u32), ("num_sb", c_u32), ("sb_chunks", c_u32),
@@ -92,6 +97,9 @@ SIGNATURES = {
                                           ctypes.POINTER(c_u64)]),
     "dsplat_set_stage_events": (c_i32, [ctypes.POINTER(c_void_p), c_i32]),
     "dsplat_adam_step": (c_i32, [_P, c_i64, _P, _P, _P, _P, c_f32, c_f32, c_f32, c_f32, c_i32]),
+    "dsplat_gauss_adam_step": (c_i32, [_P, c_i64, c_i32, ctypes.POINTER(GaussTensors), ctypes.POINTER(GaussGrads),
+                                       ctypes.POINTER(GaussTensors), ctypes.POINTER(GaussTensors), c_f32, c_f32,
+                                       c_f32, c_f32, _P]),
 }
 
 

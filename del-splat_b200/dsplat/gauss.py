@@ -59,8 +59,13 @@ class GaussBatch:
     """
 
     def __init__(self, num_pnt: int, cameras: Sequence[Camera], tile_size: int = 16, sh_degree: int = 3,
-                 pair_capacity: int = 1 << 20, device: Optional[torch.device] = None, pixels_per_lane: int = 0):
+                 pair_capacity: int = 1 << 20, device: Optional[torch.device] = None, pixels_per_lane: int = 0,
+                 check_overflow: bool = True):
         self.device = torch.device(device or "cuda")
+        # render() reads the overflow flag after each forward (one host sync);
+        # False keeps the forward free of host syncs (graph capture) and
+        # leaves the check to the caller (status())
+        self.check_overflow = bool(check_overflow)
         self.n = int(num_pnt)
         self.cameras = list(cameras)
         self.tile_size = int(tile_size)
@@ -213,6 +218,15 @@ class _RenderFn(torch.autograd.Function):
                       opacity=opacity.detach(), colors=colors.detach())
         out = torch.empty(int(batch.layout.num_pix) * 3, dtype=torch.float32, device=means.device)
         batch.forward(params, out_rgb=out)
+        if batch.check_overflow:
+            flags, needed, _ = batch.status()
+            if flags:  # the lists outgrew the capacity: grow once and render again
+                batch._alloc(int(needed * 1.05) + 1024)
+                batch.forward(params, out_rgb=out)
+                flags, needed, _ = batch.status()
+                if flags:
+                    raise RuntimeError(f"tile-list capacity exceeded ({needed} entries needed, "
+                                       f"{batch.capacity} available)")
         ctx.batch = batch
         ctx.save_for_backward(means, log_scales, quats, opacity, colors)
         return out
@@ -245,15 +259,47 @@ def adam_step(param: torch.Tensor, grad: torch.Tensor, exp_avg: torch.Tensor, ex
             "adam_step")
 
 
+def _tensors(d: Dict[str, torch.Tensor]) -> N.GaussTensors:
+    for k in PARAM_NAMES:
+        _require_cuda(d[k], k)
+    return N.GaussTensors(*(d[k].data_ptr() for k in PARAM_NAMES))
+
+
+class Adam:
+    """Fused Adam over the five parameter tensors of a scene: one
+    ``dsplat_gauss_adam_step`` launch per step, the same update as
+    ``torch.optim.Adam`` (no weight decay).  The step count lives on the
+    device, so the update can sit inside a captured CUDA graph.  Opacity is
+    kept in [0, 0.999] after every update (the blend needs alpha < 1)."""
+
+    def __init__(self, params: Dict[str, torch.Tensor], sh_degree: int, lr: float = 1e-3, betas=(0.9, 0.999),
+                 eps: float = 1e-8):
+        self.params, self.sh_degree = params, int(sh_degree)
+        self.lr, self.betas, self.eps = float(lr), (float(betas[0]), float(betas[1])), float(eps)
+        self.exp_avg = {k: torch.zeros_like(v) for k, v in params.items()}
+        self.exp_avg_sq = {k: torch.zeros_like(v) for k, v in params.items()}
+        self.step_count = torch.zeros(1, dtype=torch.int32, device=params["means"].device)
+
+    def step(self, grads: Dict[str, torch.Tensor]) -> None:
+        p = self.params
+        g = N.GaussGrads(*(grads[k].data_ptr() for k in PARAM_NAMES))
+        N.check(N.lib().dsplat_gauss_adam_step(
+            _stream_ptr(p["means"].device), p["means"].shape[0], self.sh_degree, ctypes.byref(_tensors(p)),
+            ctypes.byref(g), ctypes.byref(_tensors(self.exp_avg)), ctypes.byref(_tensors(self.exp_avg_sq)),
+            self.lr, self.betas[0], self.betas[1], self.eps, self.step_count.data_ptr()), "gauss_adam_step")
+
+
 class CapturedStep:
-    """A whole batched training step (zero grads, forward with L2 loss, backward)
-    captured into one CUDA graph.  The batch's forward has no host
-    synchronisation (fixed list capacity, overflow reported by a device flag),
-    so the step replays with zero host work per kernel."""
+    """A whole batched training step (zero grads, forward with L2 loss,
+    backward, and the optimizer's update when one is given) captured into one
+    CUDA graph.  The batch's forward has no host synchronisation (fixed list
+    capacity, overflow reported by a device flag), so the step replays with
+    zero host work per kernel."""
 
     def __init__(self, batch: GaussBatch, params: Dict[str, torch.Tensor], grads: Dict[str, torch.Tensor],
-                 target: torch.Tensor, warmup: int = 2):
+                 target: torch.Tensor, warmup: int = 2, optimizer: Optional[Adam] = None):
         self.batch, self.params, self.grads, self.target = batch, params, grads, target
+        self.optimizer = optimizer
         side = torch.cuda.Stream(batch.device)
         side.wait_stream(torch.cuda.current_stream(batch.device))
         with torch.cuda.stream(side):
@@ -271,6 +317,8 @@ class CapturedStep:
             g.zero_()
         self.batch.forward(self.params, target=self.target)
         self.batch.backward(self.params, self.grads)
+        if self.optimizer is not None:
+            self.optimizer.step(self.grads)
 
     def replay(self):
         self.graph.replay()

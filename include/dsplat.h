@@ -149,9 +149,10 @@ int dsplat_point_rasterize_pix_zbuffer(dsplat_stream stream, uint32_t num_pnt, c
  * host application owns every GPU allocation, or a loop that must not call
  * cudaMalloc): no zbuf argument and nothing is allocated; the 64-bit keys live
  * in a fixed 2^20-entry (8 MiB) array inside the library, so img_w*img_h must
- * be <= 1048576 (larger images return DSPLAT_ERR_INVALID_ARG).  The first call
- * on a device looks the array up; make it before any stream capture.  Calls
- * share the array: calls whose GPU work overlaps race. */
+ * be <= 1048576 (larger images return DSPLAT_ERR_INVALID_ARG).  Each call
+ * looks the array's address up on the current device; the first call on a
+ * device also loads the library there, so make it before any stream capture.
+ * Calls share the array: calls whose GPU work overlaps race. */
 int dsplat_point_rasterize_pix_zbuffer_noalloc(dsplat_stream stream, uint32_t num_pnt, const float* pnt2pixxyndcz,
                                                const float* pnt2rgb, float* pix2rgb, float* pix2unitdepth,
                                                int32_t* pix2winner, uint32_t img_w, uint32_t img_h);
@@ -207,7 +208,7 @@ typedef struct {
   uint32_t slabs_per_tile; /* raster warp tasks per tile (4 for 32x32 tiles, else 1) */
   uint32_t num_sb;    /* superblocks over all views */
   uint32_t sb_chunks; /* entries of sb_start per superblock */
-  size_t off_flags;      /* u32[16]: [0] flags, [1] tile pairs, [4] superblock entries */
+  size_t off_flags;      /* u32[16]: [0] flags, [6..7] tile pairs (u64), [8..9] superblock entries (u64) */
   size_t off_rec;        /* float4[V*N*3] per-view 2D records (written where the tile span is not empty) */
   size_t off_rect;       /* uint2[V*N] tile spans */
   size_t off_cnt;        /* u32[V*N] reserved (tiles per point; not written by the batched forward) */
@@ -259,6 +260,26 @@ int dsplat_gauss_batch_status(dsplat_stream stream, const void* workspace, uint3
  * ready, 5 rasterised; backward 6 start, 7 gradients cleared, 8 backward
  * raster done, 9 projection backward done.  count 0 disables. */
 int dsplat_set_stage_events(void* const* events, int32_t count);
+
+/* Mutable parameter tensors (same shapes as dsplat_gauss_params). */
+typedef struct {
+  float* means;
+  float* log_scales;
+  float* quats;
+  float* opacity;
+  float* colors;
+} dsplat_gauss_tensors;
+
+/* No reference counterpart (the reference does not train).  One fused Adam
+ * update of all five parameter tensors, the form torch.optim.Adam computes
+ * (no weight decay): step is a device int32 holding the number of updates
+ * done so far; the call uses step + 1 for the bias corrections and stores it,
+ * so a captured graph replays with the right count.  Opacity is kept in
+ * [0, 0.999] after the update (the blend needs alpha < 1). */
+int dsplat_gauss_adam_step(dsplat_stream stream, int64_t num_pnt, int32_t sh_degree,
+                           const dsplat_gauss_tensors* params, const dsplat_gauss_grads* grads,
+                           const dsplat_gauss_tensors* exp_avg, const dsplat_gauss_tensors* exp_avg_sq, float lr,
+                           float beta1, float beta2, float eps, int32_t* step);
 
 /* Adam (bias-corrected) on one parameter tensor, in place. */
 int dsplat_adam_step(dsplat_stream stream, int64_t n, float* param, const float* grad, float* exp_avg,

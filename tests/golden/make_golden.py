@@ -4,7 +4,11 @@ the del-splat sources exist; the outputs are committed).
 The expected values come from the reference's own CUDA sources compiled as
 host C++ (oracle/ref/: tile_acceleration.h for tile lists and keys,
 splat_point.cu for the point z-buffer); the inputs are seeded synthetic
-projections.  Usage: python tests/golden/make_golden.py
+projections.  bulba_subset.ply is a seeded 3,000-row subset of the
+reference's 3DGS capture asset/bulba.ply (header kept, vertex count
+adjusted), the real-data input of the PLY reader and render tests.
+Usage: python tests/golden/make_golden.py [del-splat checkout]
+(default: $DSPLAT_REFERENCE_ROOT, else /root/reference)
 """
 import os
 import sys
@@ -19,8 +23,34 @@ import oracle  # noqa: E402
 from dsplat import scenes  # noqa: E402
 
 
+def reference_root() -> str:
+    if len(sys.argv) > 1:
+        return sys.argv[1]
+    return os.environ.get("DSPLAT_REFERENCE_ROOT", "/root/reference")
+
+
+def bulba_subset(rows: int = 3000, seed: int = 17) -> None:
+    src = os.path.join(reference_root(), "asset", "bulba.ply")
+    with open(src, "rb") as f:
+        head = []
+        while True:
+            line = f.readline()
+            head.append(line)
+            if line == b"end_header\n":
+                break
+        body = f.read()
+    n = next(int(l.split()[2]) for l in head if l.startswith(b"element vertex"))
+    rec = np.frombuffer(body, dtype="<f4").reshape(n, -1)
+    keep = np.sort(np.random.default_rng(seed).choice(n, rows, replace=False))
+    head = [b"element vertex %d\n" % rows if l.startswith(b"element vertex") else l for l in head]
+    with open(os.path.join(HERE, "bulba_subset.ply"), "wb") as f:
+        f.write(b"".join(head))
+        f.write(np.ascontiguousarray(rec[keep]).tobytes())
+
+
 def main():
-    oracle.build()
+    oracle.build(reference_root())
+    bulba_subset()
     assert oracle.ref_available(), "oracle/_ref missing: needs the del-splat tree"
     # Gaussians: 2048 points, 120x72 image, 8-pixel tiles
     sc = scenes.config0(seed=11, n=2048, size=(120, 72))

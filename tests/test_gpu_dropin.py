@@ -163,3 +163,42 @@ def test_point_zbuffer_matches_painter_and_reference(orc, dev):
     assert np.array_equal(F(pix)[hit], d["rgb_out"][hit])
     win = orc.point_render_sort_depth(d["xyd"], w, h)
     assert np.array_equal(win >= 0, hit)
+
+
+def _config1_zbuffer(orc, dev, n, size):
+    """Config 1's circle z-buffer (u32 RGBA, pixel radius 1..4) on the GPU and
+    the oracle's tiled painter (splat_circle.cu:93-132 order: the nearest
+    covering point wins, ties to the larger index)."""
+    w, h = size
+    pts = scenes.config1(n=n, size=size)
+    m = pts.xyz.shape[0]
+    xyd = torch.empty((m, 3), device=dev)
+    rad0 = torch.empty((m,), device=dev)
+    cudarc.splat_circle_pnt2splat3_to_pnt2splat2(None, T(pts.xyz, dev), xyd, rad0, T(pts.camera.mvp, dev), size,
+                                                 0.0)
+    rad = T(pts.radius_px, dev)
+    rgba = T(pts.rgba.view(np.int32), dev)
+    pix, win = cudarc.circle_splat_zbuffer(None, size, xyd, rad, rgba, 16, want_winner=True)
+    oxyd, _ = orc.circle_project(pts.xyz, pts.camera.mvp, w, h, 0.0)
+    assert np.array_equal(F(xyd).view(np.uint32), oxyd.view(np.uint32))
+    aabb = orc.circle_aabb(oxyd, pts.radius_px)
+    t2i, i2p, _ = orc.tile2pnt(oxyd, aabb, w, h, 16, with_keys=False)
+    o_win = orc.circle_splat_tiled(w, h, 16, t2i, i2p, oxyd, pts.radius_px)
+    expect = np.where(o_win >= 0, pts.rgba[np.maximum(o_win, 0)], 0).astype(np.uint32)
+    return F(pix).view(np.uint32), F(win), expect, o_win
+
+
+def test_circle_zbuffer_u32_rgba_small(orc, dev):
+    pix, win, expect, o_win = _config1_zbuffer(orc, dev, 40000, (160, 120))
+    assert (o_win >= 0).sum() > 1000
+    assert np.array_equal(win, o_win)
+    assert np.array_equal(pix, expect)
+
+
+def test_circle_zbuffer_config1_full_size(orc, dev):
+    """Config 1 itself: 1,048,576 points, 1024x1024, radius 1..4 px, u32 RGBA;
+    winners and pixels bit-exact."""
+    pix, win, expect, o_win = _config1_zbuffer(orc, dev, 1 << 20, (1024, 1024))
+    assert (o_win >= 0).mean() > 0.5
+    assert np.array_equal(win, o_win)
+    assert np.array_equal(pix, expect)

@@ -195,3 +195,34 @@ def test_thousands_of_superblocks_take_the_unstaged_scatter(orc, dev):
     batch.ensure_capacity(p)
     assert batch.status()[0] == 0
     _check_view(orc, batch, sc, 0, 8)
+
+
+def test_headline_batch_matches_plain_and_oracle(orc, dev):
+    """The benchmarked batch (config 3: 1,048,576 Gaussians, SH 3, 16 views of
+    mixed resolution) in one batched forward, against the plain per-view path
+    on every view (max-abs <= 1e-4; observed bit-exact) and against the oracle
+    on the first view and the first 1920x1080 view."""
+    sc = scenes.config3(n=1 << 20, views=16)
+    p = params_of(sc, dev)
+    batch = GaussBatch(sc.n, sc.cameras, 8, 3, pair_capacity=1 << 26, device=dev)
+    batch.ensure_capacity(p)
+    batch.forward(p)
+    imgs = [F(x) for x in batch.images()]
+    worst = 0.0
+    for v, cam in enumerate(sc.cameras):
+        one = GaussBatch(sc.n, [cam], 8, 3, pair_capacity=1 << 24, device=dev)
+        one.ensure_capacity(p)
+        one.forward(p)
+        worst = max(worst, float(np.abs(F(one.images()[0]) - imgs[v]).max()))
+        del one
+    print(f"headline batch vs plain per-view: max|img| {worst:.3g}")
+    assert worst <= IMG_TOL
+    big = next(v for v, c in enumerate(sc.cameras) if c.width == 1920)
+    for v in sorted({0, big}):
+        cam = sc.cameras[v]
+        xyd, conic, aabb, rgb = orc.fused_project(sc.means, sc.log_scales, sc.quats, sc.colors, 3, cam.mvp,
+                                                  cam.campos, cam.width, cam.height)
+        t2i, i2p, _ = orc.tile2pnt(xyd, aabb, cam.width, cam.height, 16, with_keys=False)
+        o_img, _, _ = orc.gauss_rasterize_tiled(cam.width, cam.height, 16, t2i, i2p, xyd, conic, aabb, sc.opacity,
+                                                rgb, nthreads=16)
+        assert np.array_equal(imgs[v], o_img)
