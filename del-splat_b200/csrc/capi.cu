@@ -68,7 +68,7 @@ cudaError_t expf_cr_launch(cudaStream_t, size_t, const float*, float*);
 cudaError_t circle_splat_tiles(cudaStream_t, int, int, int, float*, const float*, const float*, const float*,
                                const uint32_t*, const uint32_t*);
 
-__global__ void k_adam_fused(AdamSeg, float, float, float, float, const int32_t*);
+__global__ void k_adam_fused(AdamSeg, double, double, double, double, const int32_t*);
 __global__ void k_adam_step_inc(int32_t*);
 
 __global__ void k_one_minus(const float* __restrict__ T, float* __restrict__ out, size_t n) {
@@ -837,8 +837,8 @@ int dsplat_gauss_batch_status(dsplat_stream stream, const void* workspace, uint3
 
 int dsplat_gauss_adam_step(dsplat_stream stream, int64_t num_pnt, int32_t sh_degree,
                            const dsplat_gauss_tensors* params, const dsplat_gauss_grads* grads,
-                           const dsplat_gauss_tensors* exp_avg, const dsplat_gauss_tensors* exp_avg_sq, float lr,
-                           float beta1, float beta2, float eps, int32_t* step) {
+                           const dsplat_gauss_tensors* exp_avg, const dsplat_gauss_tensors* exp_avg_sq, double lr,
+                           double beta1, double beta2, double eps, int32_t* step) {
   if (num_pnt <= 0) return DSPLAT_OK;
   if (!params || !grads || !exp_avg || !exp_avg_sq || !step) return fail(DSPLAT_ERR_INVALID_ARG, "null argument");
   if (sh_degree < -1 || sh_degree > 3) return fail(DSPLAT_ERR_INVALID_ARG, "sh_degree must be -1..3");

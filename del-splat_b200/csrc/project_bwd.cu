@@ -385,28 +385,34 @@ __global__ void k_adam(size_t n, float* __restrict__ p, const float* __restrict_
 // Fused Adam over the five parameter tensors of a Gaussian scene (one
 // launch), with the step count kept on the device so that a captured graph
 // replays correctly: every thread reads t = *step + 1 and k_adam_step_inc
-// stores it after the update.  Same update as torch.optim.Adam (no weight
-// decay, no amsgrad): m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2,
-// p -= lr (m / (1 - b1^t)) / (sqrt(v / (1 - b2^t)) + eps).  The opacity
-// tensor is then kept in [0, kOpacityMax]: the blend needs alpha < 1 (the
-// backward rebuilds T in front of an entry as T / (1 - alpha)).
+// stores it after the update.  The update is torch.optim.Adam's (no weight
+// decay, no amsgrad), in its order: m += (1-b1)(g - m); v = v b2 + (1-b2) g^2;
+// p -= (lr / (1 - b1^t)) m / (sqrt(v) / sqrt(1 - b2^t) + eps), with the
+// hyper-parameters and bias corrections formed in double and rounded to
+// float as torch rounds its Python scalars.  The opacity tensor is then kept
+// in [0, kOpacityMax]: the blend needs alpha < 1 (the backward rebuilds T in
+// front of an entry as T / (1 - alpha)).
 constexpr float kOpacityMax = 0.999f;
 
-__global__ void k_adam_fused(AdamSeg seg, float lr, float b1, float b2, float eps, const int32_t* __restrict__ step) {
+__global__ void k_adam_fused(AdamSeg seg, double lr, double b1, double b2, double eps,
+                             const int32_t* __restrict__ step) {
   const size_t total = seg.end[4];
-  const float t = float(*step + 1);
-  const float bc1 = 1.f - powf(b1, t), bc2 = 1.f - powf(b2, t);
+  const double t = double(*step + 1);
+  const float step_size = float(lr / (1.0 - pow(b1, t)));
+  const float bc2_sqrt = float(sqrt(1.0 - pow(b2, t)));
+  const float w1 = float(1.0 - b1), b2f = float(b2), w2 = float(1.0 - b2), epsf = float(eps);
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
     int k = 0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) k += i >= seg.end[j];
     const size_t o = i - (k ? seg.end[k - 1] : 0);
     const float gi = seg.g[k][o];
-    const float mi = b1 * seg.m[k][o] + (1.f - b1) * gi;
-    const float vi = b2 * seg.v[k][o] + (1.f - b2) * gi * gi;
+    const float mi = seg.m[k][o] + w1 * (gi - seg.m[k][o]);
+    const float vi = seg.v[k][o] * b2f + w2 * (gi * gi);
     seg.m[k][o] = mi;
     seg.v[k][o] = vi;
-    float pi = seg.p[k][o] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    const float denom = sqrtf(vi) / bc2_sqrt + epsf;
+    float pi = seg.p[k][o] - step_size * (mi / denom);
     if (k == 3) pi = fminf(fmaxf(pi, 0.f), kOpacityMax);
     seg.p[k][o] = pi;
   }

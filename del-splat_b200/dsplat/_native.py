@@ -98,8 +98,8 @@ SIGNATURES = {
     "dsplat_set_stage_events": (c_i32, [ctypes.POINTER(c_void_p), c_i32]),
     "dsplat_adam_step": (c_i32, [_P, c_i64, _P, _P, _P, _P, c_f32, c_f32, c_f32, c_f32, c_i32]),
     "dsplat_gauss_adam_step": (c_i32, [_P, c_i64, c_i32, ctypes.POINTER(GaussTensors), ctypes.POINTER(GaussGrads),
-                                       ctypes.POINTER(GaussTensors), ctypes.POINTER(GaussTensors), c_f32, c_f32,
-                                       c_f32, c_f32, _P]),
+                                       ctypes.POINTER(GaussTensors), ctypes.POINTER(GaussTensors),
+                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P]),
 }
 
 

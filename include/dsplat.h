@@ -278,8 +278,8 @@ typedef struct {
  * [0, 0.999] after the update (the blend needs alpha < 1). */
 int dsplat_gauss_adam_step(dsplat_stream stream, int64_t num_pnt, int32_t sh_degree,
                            const dsplat_gauss_tensors* params, const dsplat_gauss_grads* grads,
-                           const dsplat_gauss_tensors* exp_avg, const dsplat_gauss_tensors* exp_avg_sq, float lr,
-                           float beta1, float beta2, float eps, int32_t* step);
+                           const dsplat_gauss_tensors* exp_avg, const dsplat_gauss_tensors* exp_avg_sq, double lr,
+                           double beta1, double beta2, double eps, int32_t* step);
 
 /* Adam (bias-corrected) on one parameter tensor, in place. */
 int dsplat_adam_step(dsplat_stream stream, int64_t n, float* param, const float* grad, float* exp_avg,

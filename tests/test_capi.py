@@ -116,3 +116,39 @@ def test_plain_c_client_builds_and_runs(tmp_path):
     run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert run.returncode == 0, run.stdout + run.stderr
     assert "sm_100a" in run.stdout and "rejected" in run.stdout
+
+
+def _c_decls():
+    """name -> number of parameters, for every entry point in include/*.h."""
+    out = {}
+    for f in os.listdir(os.path.join(ROOT, "include")):
+        if not f.endswith(".h"):
+            continue
+        src = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", f)).read(), flags=re.S)
+        for m in re.finditer(r"(?:int|size_t|uint64_t|const char\*)\s+(dsplat_\w+)\s*\(([^)]*)\)\s*;", src):
+            args = m.group(2).strip()
+            out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_rust_shim_declarations_match_the_header():
+    """del-splat_b200/rust (the del-splat-cudarc replacement, built where cargo
+    exists) declares the C ABI by hand; every extern "C" function it declares
+    must exist in include/dsplat.h with the same number of parameters, and it
+    must cover the drop-in entry points its wrappers call."""
+    src = open(os.path.join(ROOT, "del-splat_b200", "rust", "src", "ffi.rs")).read()
+    rust = {}
+    for m in re.finditer(r"pub fn (dsplat_\w+)\s*\(([^)]*)\)", src, re.S):
+        args = [a for a in m.group(2).split(",") if a.strip()]
+        rust[m.group(1)] = len(args)
+    header = _c_decls()
+    assert len(rust) >= 17
+    for name, n in rust.items():
+        assert name in header, name
+        assert header[name] == n, (name, n, header[name])
+    wrappers = (open(os.path.join(ROOT, "del-splat_b200", "rust", "src", "splat_gauss.rs")).read() +
+                open(os.path.join(ROOT, "del-splat_b200", "rust", "src", "splat_circle.rs")).read())
+    called = set(re.findall(r"ffi::(dsplat_\w+)\(", wrappers))
+    assert called <= set(rust)
+    for fn in ("pnt2splat3_to_pnt2splat2", "rasterize_pnt2splat2", "tile2idx_idx2pnt", "splat"):
+        assert re.search(r"pub fn " + fn + r"\(", wrappers), fn

@@ -61,7 +61,7 @@ def test_colmap_views_render(orc, dev, tmp_path):
 def test_circle_splat_from_project_spheres_and_torch_wrapper(orc, dev):
     """del-splat-dlpack/src/splat_circle.rs:11-75 (module function and
     SplatCircle.torch.from_project_spheres) against the oracle's projection."""
-    import del_splat_dlpack
+    from del_splat_dlpack import del_splat_dlpack
     from del_splat_dlpack.SplatCircle import torch as sct
     pts = scenes.config1(n=40000, size=(320, 240))
     n = pts.xyz.shape[0]

@@ -106,8 +106,15 @@ def test_config0_cuda_stop_rule_against_reference_kernel(orc, dev):
 
 def test_1080p_sh3_view_against_del_splat_cpu(orc, dev):
     """One 1920x1080 view of the 1,048,576-Gaussian SH-3 scene (config 3)
-    through the batched path, against del-splat-cpu's blend on the oracle's
-    projection and tile lists."""
+    through the batched path.  Against the oracle (correctly rounded exp):
+    bit-exact.  Against del-splat-cpu's literal arithmetic (glibc expf, which
+    is not correctly rounded on about 1 input in 11,500): every pixel whose
+    walk stops at the same entry is within 1e-4; the stop test is a threshold,
+    so a last-bit difference in the alpha sum next to 0.999 can move the stop
+    by one entry on a handful of pixels (each then differs by that entry's
+    contribution, T ~ 1e-3 times its alpha).  Their share is printed and
+    bounded, next to the reference's own disagreement between its CUDA stop
+    test and del-splat-cpu's on the same view."""
     sc = scenes.config3(n=1 << 20, views=16)
     cam = next(c for c in sc.cameras if c.width == 1920)
     sc.cameras = [cam]
@@ -126,9 +133,17 @@ def test_1080p_sh3_view_against_del_splat_cpu(orc, dev):
     assert np.array_equal(img.view(np.uint32), o_img.view(np.uint32))
     assert np.array_equal(Tm.view(np.uint32), o_T.view(np.uint32))
     c_img, c_T, c_stop = orc.gauss_rasterize_tiled(*args, nthreads=16, mode=orc.BLEND_LIBM_EXP)
-    d_img = float(np.abs(img - c_img).max())
-    d_alpha = float(np.abs(Tm - c_T).max())
-    moved = float((o_stop != c_stop).mean())
-    print(f"1080p SH3 vs del-splat-cpu: max|img| {d_img:.3g}, max|alpha| {d_alpha:.3g}, "
-          f"stop position differs on {moved:.2e} of pixels")
+    same = o_stop == c_stop
+    d_img = float(np.abs(img - c_img).max(axis=2)[same].max())
+    d_alpha = float(np.abs(Tm - c_T)[same].max())
+    moved = float((~same).mean())
+    k_img, _, k_stop = orc.gauss_rasterize_tiled(*args, nthreads=16,
+                                                 mode=orc.BLEND_LIBM_EXP | orc.BLEND_CUDA_STOP)
+    ref_moved = float((k_stop != c_stop).mean())
+    ref_over = int((np.abs(k_img - c_img).max(axis=2) > TOL).sum())
+    print(f"1080p SH3 vs del-splat-cpu: stop positions agree on {same.mean():.7f} of pixels, there max|img| "
+          f"{d_img:.3g}, max|alpha| {d_alpha:.3g}; moved {moved:.2e} (max|img| overall "
+          f"{float(np.abs(img - c_img).max()):.3g}); the reference's CUDA stop test vs del-splat-cpu: moved "
+          f"{ref_moved:.2e}, {ref_over} pixels beyond 1e-4")
     assert d_img <= TOL and d_alpha <= TOL
+    assert moved <= 1e-5
