@@ -147,21 +147,77 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- helpers
-def profiled_traffic(kernel_stage: str, views: int):
-    """DRAM bytes per launch of a stage's kernel: the per-view figure of the
-    committed ncu summary (profiles/*.md line `traffic_per_view_bytes <kernel>
-    <bytes>`) times the views of this launch; None when not profiled."""
+def source_hash() -> str:
+    """SHA-256 over the CUDA sources and the C header: the build an ncu
+    capture in profiles/ belongs to."""
+    import hashlib
+    h = hashlib.sha256()
+    csrc = os.path.join(PKG, "csrc")
+    files = sorted(f for f in os.listdir(csrc) if f.endswith((".cu", ".cuh")))
+    for f in files:
+        with open(os.path.join(csrc, f), "rb") as fh:
+            h.update(f.encode() + b"\0" + fh.read())
+    with open(os.path.join(ROOT, "include", "dsplat.h"), "rb") as fh:
+        h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+KERNEL_OF_STAGE = {"raster_fwd": "k_raster_fwd", "raster_bwd": "k_raster_bwd", "sb_lists": "k_sb_scatter_staged",
+                   "project_bwd": "k_project_bwd_colour", "project_fwd": "k_fused_project"}
+
+
+def captured_figures(stage: str, workload: str):
+    """Per-launch figures of a stage's kernel from the committed ncu summary
+    of this very build: lines `capture_build <hash>`, `workload <text>` and
+    `per_launch <workload> <kernel> inst <warp-instructions> dram_bytes
+    <bytes>` in a profiles/*.md.  None when no capture of the current sources
+    exists (the line then says so instead of reporting a stale figure)."""
     import glob
     import re
-    kernel = {"raster_bwd": "k_raster_bwd", "raster_fwd": "k_raster_fwd"}.get(kernel_stage)
+    kernel = KERNEL_OF_STAGE.get(stage)
     if kernel is None:
         return None
+    want = source_hash()
     for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
         with open(path) as f:
-            m = re.search(r"traffic_per_view_bytes\s+" + kernel + r"\s+(\d+)", f.read())
-        if m:
-            return int(m.group(1)) * views
+            txt = f.read()
+        m_build = re.search(r"capture_build\s+([0-9a-f]+)", txt)
+        m = re.search(r"per_launch\s+" + workload + r"\s+" + kernel + r"\s+inst\s+(\d+)\s+dram_bytes\s+(\d+)", txt)
+        if m and m_build and m_build.group(1) == want:
+            wl = re.search(r"workload\s+(.+)", txt)
+            return {"inst": int(m.group(1)), "dram_bytes": int(m.group(2)),
+                    "capture": os.path.relpath(path, ROOT), "workload": wl.group(1).strip() if wl else None}
     return None
+
+
+def num_sms(dev) -> int:
+    return int(torch.cuda.get_device_properties(dev).multi_processor_count)
+
+
+def issue_roofline(stage: str, launch_ms: float, clocks: dict, dev, hbm_peak: float, peak_kind: str,
+                   workload: str = "gauss-batch") -> dict:
+    """Instruction-issue roofline of one launch of `stage`'s kernel: warp-
+    instructions per launch (ncu capture of this build) / this run's CUDA-
+    event launch time, against 4 warp-instructions per clock per SM at this
+    run's median sampled SM clock; the capture's DRAM bytes per launch give
+    the HBM fraction beside it."""
+    fig = captured_figures(stage, workload)
+    clk = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    ceiling = num_sms(dev) * 4 * clk * 1e6 / 1e9  # G warp-instructions/s
+    out = {"kernel": KERNEL_OF_STAGE.get(stage, stage), "stage": stage, "bound": "issue",
+           "unit": "G warp-instructions/s", "peak": ceiling, "launch_ms": launch_ms,
+           "peak_note": f"{num_sms(dev)} SMs x 4 schedulers x {clk:.0f} MHz (median SM clock sampled in the run)"}
+    if fig is None:
+        out.update({"achieved": None, "frac": None, "traffic": None,
+                    "note": "no ncu capture of this build in profiles/ (source hash " + source_hash() + ")"})
+        return out
+    achieved = fig["inst"] / (launch_ms / 1e3) / 1e9
+    gbs = fig["dram_bytes"] / (launch_ms / 1e3) / 1e9
+    out.update({"achieved": achieved, "frac": achieved / ceiling, "traffic": fig["dram_bytes"],
+                "inst_per_launch": fig["inst"], "capture": fig["capture"], "capture_workload": fig["workload"],
+                "hbm": {"achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+                        "peak_kind": peak_kind}})
+    return out
 
 
 def cpu_model() -> str:
@@ -426,12 +482,39 @@ def run_zbuffer(args, rank, world, local):
             "gpu_launches": int(launches), "clocks": clk.summary()}), flush=True)
 
 
+STAGE_NAMES = ["project_fwd", "depth_sort", "sb_lists", "task_order", "raster_fwd", "(host gap)", "grad_clear",
+               "raster_bwd", "project_bwd"]
+
+
+def measure_stages(L, step, steps: int) -> np.ndarray:
+    """Mean per-stage times (ms, CUDA events recorded on the launch stream by
+    the library's stage hook) of `steps` eager runs of step()."""
+    from dsplat import _native
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(10)]
+    for e in evs:
+        e.record()
+    torch.cuda.synchronize()
+    handles = (_native.c_void_p * 10)(*[e.cuda_event for e in evs])
+    stage_ms = np.zeros(9)
+    for _ in range(steps):
+        L.dsplat_set_stage_events(handles, 10)
+        step()
+        L.dsplat_set_stage_events(None, 0)
+        torch.cuda.synchronize()
+        stage_ms += [evs[i].elapsed_time(evs[i + 1]) for i in range(9)]
+    return stage_ms / max(steps, 1)
+
+
 def run_train4m(args, rank, world, local):
     """4,194,304 Gaussians (SH 3), 8 views at 1920x1080, one training step =
-    forward with L2 loss + backward + Adam (lr 1e-3, betas 0.9/0.999) on all
-    parameters."""
+    forward with L2 loss + backward + fused Adam (lr 1e-3, betas 0.9/0.999)
+    on all parameters, captured in one CUDA graph with the Adam step count
+    on the device.  e2e: each step's target images come from pinned host
+    memory and its loss goes back (the parameters live on the device, as in
+    training)."""
     from dsplat import _native, scenes
-    from dsplat.gauss import GaussBatch, adam_step
+    from dsplat.feed import DeviceToHostDrain, HostToDeviceFeed
+    from dsplat.gauss import Adam, CapturedStep, GaussBatch
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     L = _native.lib()
@@ -440,58 +523,137 @@ def run_train4m(args, rank, world, local):
             "colors": sc.colors.reshape(sc.n, -1)}
     params = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in host.items()}
     grads = {k: torch.zeros_like(v) for k, v in params.items()}
-    m1 = {k: torch.zeros_like(v) for k, v in params.items()}
-    m2 = {k: torch.zeros_like(v) for k, v in params.items()}
     tgt = np.concatenate([t.reshape(-1) for t in scenes.targets_for(sc, seed=99 + rank)])
     target = torch.from_numpy(tgt).to(dev)
     ts, ppl = (args.tile, args.ppl) if args.tile else (8, 2)
-    batch = GaussBatch(sc.n, sc.cameras, ts, 3, pair_capacity=1 << 26, device=dev, pixels_per_lane=ppl)
+    batch = GaussBatch(sc.n, sc.cameras, ts, 3, pair_capacity=1 << 26, device=dev, pixels_per_lane=ppl,
+                       check_overflow=False)
     batch.ensure_capacity(params)
-    step_no = [0]
+    V = len(sc.cameras)
 
-    def step():
+    # untimed parity check before any update: the batched images against the
+    # plain per-view path (each view rendered alone), max-abs
+    batch.forward(params)
+    imgs = batch.images()
+    worst = 0.0
+    for v, cam in enumerate(sc.cameras):
+        one = GaussBatch(sc.n, [cam], ts, 3, pair_capacity=1 << 25, device=dev, pixels_per_lane=ppl)
+        one.ensure_capacity(params)
+        one.forward(params)
+        worst = max(worst, float((one.images()[0] - imgs[v]).abs().max()))
+        del one
+    torch.cuda.empty_cache()
+
+    def eager_step(opt):
         for g in grads.values():
             g.zero_()
         batch.forward(params, target=target)
         batch.backward(params, grads)
-        step_no[0] += 1
-        for k in params:
-            adam_step(params[k], grads[k], m1[k], m2[k], 1e-3, 0.9, 0.999, 1e-8, step_no[0])
+        opt.step(grads)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    flags, _, pairs = batch.status()
+    # stage times (one eager pass per timed step, on a throw-away optimizer
+    # state; the parameters are reset afterwards)
+    snapshot = {k: v.clone() for k, v in params.items()}
+    scratch = Adam(params, 3, lr=1e-3, betas=(0.9, 0.999), eps=1e-8)
+    stage_ms = measure_stages(L, lambda: eager_step(scratch), max(1, min(args.steps, 5)))
+    for k in params:
+        params[k].copy_(snapshot[k])
+    del scratch, snapshot
+
+    adam = Adam(params, 3, lr=1e-3, betas=(0.9, 0.999), eps=1e-8)
+    graph = CapturedStep(batch, params, grads, target, warmup=args.warmup, optimizer=adam)
+    flags, _, _ = batch.status()
     if flags:
-        batch.ensure_capacity(params)
-        step()
-        torch.cuda.synchronize()
+        raise RuntimeError("pair capacity overflow in the warm-up")
     c0 = L.dsplat_launch_count()
+    eager_step(adam)  # one more real step, to count this library's launches per step
+    torch.cuda.synchronize()
+    per_step_launches = L.dsplat_launch_count() - c0
     barrier(world)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         e0.record()
         for _ in range(args.steps):
-            step()
+            graph.replay()
         e1.record()
         torch.cuda.synchronize()
-    launches = L.dsplat_launch_count() - c0
     flags, _, pairs = batch.status()
     if flags:
         raise RuntimeError("pair capacity overflow inside the timed region")
     t_ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
-    V = len(sc.cameras)
+    clocks = clk.summary()
+
+    # end to end: targets in, loss out, every step (graphs per feed slot)
+    tgt_pinned = target.cpu().pin_memory()
+    feed = HostToDeviceFeed({"target": tgt_pinned}, dev)
+    loss_dev = [torch.zeros(1, device=dev) for _ in feed.slots]
+    drain = DeviceToHostDrain({"loss": loss_dev[0]}, dev, slots=len(feed.slots))
+    for sl in feed.slots:
+        sl["target"].copy_(target)
+    slot_graphs = [CapturedStep(batch, params, grads, sl["target"], warmup=1, optimizer=adam) for sl in feed.slots]
+
+    def run_e2e(steps):
+        feed.put({"target": tgt_pinned})
+        for k in range(steps):
+            d = feed.get()
+            i = next(j for j, sl in enumerate(feed.slots) if sl is d)
+            if k + 1 < steps:
+                feed.put({"target": tgt_pinned})
+            drain.reclaim(i)
+            slot_graphs[i].replay()
+            torch.sum(batch.slab_loss(), dim=0, keepdim=True, out=loss_dev[i])
+            drain.push(i, {"loss": loss_dev[i]})
+            feed.release()
+        for i in range(len(feed.slots)):
+            drain.wait(i)
+
+    run_e2e(max(1, args.warmup))
+    torch.cuda.synchronize()
+    barrier(world)
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record()
+    run_e2e(args.steps)
+    q1.record()
+    torch.cuda.synchronize()
+    et = max_over_ranks(q0.elapsed_time(q1), world, dev)
+
+    peak, peak_kind = peaks()
+    dom = max((n for n in STAGE_NAMES if not n.startswith("(") and n != "task_order"),
+              key=lambda n: stage_ms[STAGE_NAMES.index(n)])
+    roofline = issue_roofline(dom, float(stage_ms[STAGE_NAMES.index(dom)]), clocks, dev, peak, peak_kind,
+                              workload="train4m")
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            nth = os.cpu_count() or 1
+            t1, cam = cpu_sample(sc, 0, nth, 16)
+            cpu = {"value": 1.0 / (t1 * V), "unit": "steps/s", "cores": nth, "kind": "port",
+                   "sample": f"one fwd+bwd of one {cam.width}x{cam.height} view of the {sc.n}-Gaussian SH3 "
+                             f"scene (oracle C++ restatement, OpenMP {nth} threads), x{V} views per step; "
+                             "Adam not included", "cpu_model": cpu_model()}
+        except Exception as ex:
+            cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
+
     if rank == 0:
+        value = world * args.steps / (t_ms / 1e3)
         print(json.dumps({
-            "metric": "4M-Gaussian 8x1080p fwd+bwd+Adam steps/s (1 B200)", "value": world * args.steps / (t_ms / 1e3),
+            "metric": "4M-Gaussian 8x1080p fwd+bwd+Adam steps/s (1 B200)", "value": value,
             "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded PCG64)",
-            "config": {"workload": "4M Gaussians SH3, 8 views 1920x1080, fwd+bwd+Adam", "num_gaussians": sc.n,
-                       "views": V, "views_per_s": world * V * args.steps / (t_ms / 1e3), "tile_size": ts,
-                       "pixels_per_lane": ppl, "pairs_per_step": int(pairs)},
-            "roofline": None, "cpu_baseline": None,
-            "e2e": None, "gpu_launches": int(launches), "clocks": clk.summary()}), flush=True)
+            "config": {"workload": "4M Gaussians SH3, 8 views 1920x1080, fwd+bwd+fused Adam, CUDA graph",
+                       "num_gaussians": sc.n, "views": V, "views_per_s": world * V * args.steps / (t_ms / 1e3),
+                       "tile_size": ts, "pixels_per_lane": ppl, "pairs_per_step": int(pairs), "cuda_graph": True,
+                       "l2": "inputs larger than L2 (params 944 MB)",
+                       "stage_ms": {n: round(float(stage_ms[i]), 4) for i, n in enumerate(STAGE_NAMES)}},
+            "parity": {"batched_vs_plain_max_abs": worst, "tolerance": 1e-4,
+                       "note": "the 8 views before any update, batched vs each view rendered alone"},
+            "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": {"value": world * args.steps / (et / 1e3), "unit": "steps/s",
+                    "h2d_bytes_per_step": int(tgt_pinned.numel() * 4), "d2h_bytes_per_step": 4,
+                    "result": "targets in, loss out every step; parameters stay on the device"},
+            "gpu_launches": int(per_step_launches * args.steps), "clocks": clocks}), flush=True)
 
 
 # --------------------------------------------------------------------------- GPU arm
@@ -579,26 +741,10 @@ def main():
             b.forward(params, target=t)
             b.backward(params, grads)
 
-    # stage events (live kernel timing on the launch stream)
-    evs = [torch.cuda.Event(enable_timing=True) for _ in range(10)]
-    for e in evs:
-        e.record()
-    torch.cuda.synchronize()
-    handles = (_native.c_void_p * 10)(*[e.cuda_event for e in evs])
-
     for _ in range(args.warmup):
         step_batched()
     torch.cuda.synchronize()
-
-    # per-stage times (CUDA events on the launch stream) from an instrumented pass
-    stage_ms = np.zeros(9)
-    for _ in range(args.steps):
-        L.dsplat_set_stage_events(handles, 10)
-        step_batched()
-        L.dsplat_set_stage_events(None, 0)
-        torch.cuda.synchronize()
-        stage_ms += [evs[i].elapsed_time(evs[i + 1]) for i in range(9)]
-    stage_ms /= args.steps
+    stage_ms = measure_stages(L, step_batched, args.steps)
 
     graph = None
     if not args.no_graph:
@@ -638,6 +784,7 @@ def main():
 
     # plain per-view path, same kernels one view per call
     plain_vps = None
+    parity = {}
     plain_by_cfg = {}
     plain_cfg = None
     plain = None
@@ -657,19 +804,31 @@ def main():
         plain_by_cfg[f"ts{cfg[0]}_ppl{cfg[1]}"] = vps
         if plain_vps is None or vps > plain_vps:
             plain_vps, plain_cfg = vps, cfg
+        # untimed parity check: every view of the batched step against the
+        # same view rendered alone (same kernels, one view per call)
+        worst = 0.0
+        for v, (b, _) in enumerate(plain):
+            worst = max(worst, float((b.images()[0] - batch.images()[v]).abs().max()))
+        parity[f"batched_vs_plain_max_abs_ts{cfg[0]}_ppl{cfg[1]}"] = worst
     plain_cfgs = plain = None  # release the per-view workspaces
 
-    # end to end through the public API from pinned host buffers
+    # end to end through the public API: every step's inputs (parameters and
+    # targets) come from pinned host memory and every step's result -- the
+    # rendered images of all views and the loss -- goes back to pinned host
+    # memory.  Copies in (dsplat.feed.HostToDeviceFeed) and out
+    # (DeviceToHostDrain) run on side streams: step k+1's inputs and step
+    # k-1's images move while step k computes.
     host_pinned = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in host.items()}
     tgt_pinned = target.cpu().pin_memory()
     h2d = sum(t.numel() * 4 for t in host_pinned.values()) + tgt_pinned.numel() * 4
-    loss_host = torch.empty(1, dtype=torch.float32).pin_memory()
 
-    # every step's inputs are copied from pinned host memory; the copy for
-    # step k+1 runs on a side stream while step k computes (dsplat.feed)
-    from dsplat.feed import HostToDeviceFeed
+    from dsplat.feed import DeviceToHostDrain, HostToDeviceFeed
     host_step = dict(host_pinned, target=tgt_pinned)
     feed = HostToDeviceFeed(host_step, dev)
+    outs = [torch.empty_like(batch.out_rgb) for _ in feed.slots]
+    loss_dev = [torch.zeros(1, device=dev) for _ in feed.slots]
+    drain = DeviceToHostDrain({"images": outs[0], "loss": loss_dev[0]}, dev, slots=len(feed.slots))
+    d2h = drain.bytes_per_push()
 
     # one captured step per feed slot (the graph bakes in its slot's buffers)
     slot_graphs = None
@@ -679,58 +838,53 @@ def main():
             for name in params:
                 sl[name].copy_(params[name])
             sl["target"].copy_(target)
-        slot_graphs = [CapturedStep(batch, {name: sl[name] for name in params}, grads, sl["target"])
-                       for sl in feed.slots]
+        slot_graphs = [CapturedStep(batch, {name: sl[name] for name in params}, grads, sl["target"], out_rgb=outs[i])
+                       for i, sl in enumerate(feed.slots)]
 
     def run_e2e(steps):
         feed.put(host_step)
+        last = 0
         for k in range(steps):
             d = feed.get()
+            i = next(j for j, sl in enumerate(feed.slots) if sl is d)
             if k + 1 < steps:
                 feed.put(host_step)
+            drain.reclaim(i)
             if slot_graphs is not None:
-                slot_graphs[next(i for i, sl in enumerate(feed.slots) if sl is d)].replay()
+                slot_graphs[i].replay()
             else:
                 p = {name: d[name] for name in params}
                 zero_grads()
-                batch.forward(p, target=d["target"])
+                batch.forward(p, target=d["target"], out_rgb=outs[i])
                 batch.backward(p, grads)
-            loss_host.copy_(batch.slab_loss().sum().reshape(1), non_blocking=True)
+            torch.sum(batch.slab_loss(), dim=0, keepdim=True, out=loss_dev[i])
+            drain.push(i, {"images": outs[i], "loss": loss_dev[i]})
             feed.release()
+            last = i
+        return drain.wait(last)
 
     run_e2e(args.warmup)
     torch.cuda.synchronize()
     barrier(world)
     q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     q0.record()
-    run_e2e(args.steps)
+    result = run_e2e(args.steps)
+    for i in range(len(feed.slots)):  # every readback has landed
+        drain.wait(i)
     q1.record()
     torch.cuda.synchronize()
     et = max_over_ranks(q0.elapsed_time(q1), world, dev)
     e2e_vps = world * V * args.steps / (et / 1e3)
+    e2e_images_equal = bool(torch.equal(result["images"], batch.out_rgb.cpu()))
 
-    # roofline of the dominant kernel (algorithmic bytes per launch / event time)
+    # roofline of the dominant kernel: instruction issue (the rasterisers are
+    # issue-bound with DRAM nearly idle); see issue_roofline
     peak, peak_kind = peaks()
     npix = int(batch.layout.num_pix)
-    names = ["project_fwd", "depth_sort", "sb_lists", "task_order", "raster_fwd", "(host gap)",
-             "grad_clear", "raster_bwd", "project_bwd"]
-    s_sh = 48
-    bytes_alg = {
-        "project_fwd": base.n * (40 + 4 + 4 * s_sh) + V * base.n * (48 + 8 + 4 + 4),
-        "depth_sort": 4 * V * batch.layout.npad * 16,
-        "task_order": 0,
-        "sb_lists": 2 * V * batch.layout.npad * 12,
-        "raster_fwd": pairs * 40 + npix * 20,
-        "raster_bwd": npix * 20 + pairs * 40 + V * base.n * 36,
-        "project_bwd": base.n * (40 + 4 * s_sh) + V * base.n * 48 + base.n * (40 + 4 * s_sh),
-        "grad_clear": V * base.n * 48,
-        "(host gap)": 0,
-    }
+    names = STAGE_NAMES
     dom = max((n for n in names if not n.startswith("(") and n != "task_order"),
               key=lambda n: stage_ms[names.index(n)])
-    dom_ms = stage_ms[names.index(dom)]
-    achieved = bytes_alg[dom] / (dom_ms / 1e3) / 1e9
-    traffic = profiled_traffic(dom, V)
+    roofline = issue_roofline(dom, float(stage_ms[names.index(dom)]), clocks, dev, peak, peak_kind)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -764,17 +918,13 @@ def main():
                        "l2": "inputs larger than L2 (params 236 MB, pair lists > 1 GB)",
                        "parallelism": f"replicas x{world} (views sharded, no collective)",
                        "stage_ms": {n: round(float(stage_ms[i]), 4) for i, n in enumerate(names)}},
-            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "alg_bytes_per_launch": int(bytes_alg[dom]), "launch_ms": float(dom_ms),
-                         "note": ("achieved = per-view algorithmic bytes (pixels x 20 + pairs x 40 + points x 36 "
-                                  "for the backward) / CUDA-event time; pairs are counted once per tile, as a "
-                                  "per-tile-list design would read them, while this kernel reads point records "
-                                  "through L2 and shared memory: traffic (DRAM bytes per launch, ncu, scaled "
-                                  "by views from the committed profile) shows the rasterisers are not HBM-bound "
-                                  "but instruction-issue bound (79% of issue slots busy, top stall not-selected)")},
+            "parity": dict(parity, batched_vs_plain_max_abs=max(parity.values()) if parity else None,
+                           tolerance=1e-4, note="every view's image, batched step vs the view rendered alone"),
+            "roofline": roofline,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_vps, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4},
+            "e2e": {"value": e2e_vps, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "result": "rendered images of all views + loss, to pinned host memory every step",
+                    "images_equal_resident_run": e2e_images_equal},
             "gpu_launches": int(launches),
             "clocks": clocks,
         }

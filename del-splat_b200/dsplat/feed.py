@@ -73,3 +73,56 @@ class HostToDeviceFeed:
         self.free[self.current].record(torch.cuda.current_stream(self.device))
         self.used[self.current] = True
         self.current = None
+
+
+class DeviceToHostDrain:
+    """Double-buffered device -> host readback of a step's results.
+
+    push(i, tensors) queues, on a side stream, the copy of device tensors
+    written by the work queued so far on the current stream into host slot i
+    (pinned), so the copy of step k's results runs while step k+1 computes.
+    Before the current stream overwrites those device tensors again it calls
+    reclaim(i), which makes it wait for that copy; wait(i) blocks the host
+    until slot i's copy has landed and returns its host tensors.
+
+        drain = DeviceToHostDrain({"image": dev_image}, device)
+        for k in range(steps):
+            drain.reclaim(k % 2)
+            render_into(out[k % 2])
+            drain.push(k % 2, {"image": out[k % 2]})
+        drain.wait((steps - 1) % 2)
+    """
+
+    def __init__(self, like: Dict[str, torch.Tensor], device: torch.device, slots: int = 2):
+        if slots < 1:
+            raise ValueError("slots must be >= 1")
+        self.device = torch.device(device)
+        self.copy_stream = torch.cuda.Stream(device=self.device)
+        self.host = [{k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in like.items()}
+                     for _ in range(slots)]
+        self.done = [torch.cuda.Event() for _ in range(slots)]
+        self.pending = [False] * slots
+
+    def bytes_per_push(self) -> int:
+        return sum(t.numel() * t.element_size() for t in self.host[0].values())
+
+    def reclaim(self, i: int) -> None:
+        """The current stream waits until slot i's last copy has read its
+        device tensors."""
+        if self.pending[i]:
+            torch.cuda.current_stream(self.device).wait_event(self.done[i])
+
+    def push(self, i: int, dev: Dict[str, torch.Tensor]) -> None:
+        produced = torch.cuda.Event()
+        produced.record(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(self.copy_stream):
+            self.copy_stream.wait_event(produced)
+            for k, dst in self.host[i].items():
+                dst.copy_(dev[k], non_blocking=True)
+            self.done[i].record(self.copy_stream)
+        self.pending[i] = True
+
+    def wait(self, i: int) -> Dict[str, torch.Tensor]:
+        if self.pending[i]:
+            self.done[i].synchronize()
+        return self.host[i]

@@ -297,9 +297,11 @@ class CapturedStep:
     zero host work per kernel."""
 
     def __init__(self, batch: GaussBatch, params: Dict[str, torch.Tensor], grads: Dict[str, torch.Tensor],
-                 target: torch.Tensor, warmup: int = 2, optimizer: Optional[Adam] = None):
+                 target: torch.Tensor, warmup: int = 2, optimizer: Optional[Adam] = None,
+                 out_rgb: Optional[torch.Tensor] = None):
         self.batch, self.params, self.grads, self.target = batch, params, grads, target
         self.optimizer = optimizer
+        self.out_rgb = out_rgb  # None: the batch's own image buffer
         side = torch.cuda.Stream(batch.device)
         side.wait_stream(torch.cuda.current_stream(batch.device))
         with torch.cuda.stream(side):
@@ -315,7 +317,7 @@ class CapturedStep:
     def _step(self):
         for g in self.grads.values():
             g.zero_()
-        self.batch.forward(self.params, target=self.target)
+        self.batch.forward(self.params, target=self.target, out_rgb=self.out_rgb)
         self.batch.backward(self.params, self.grads)
         if self.optimizer is not None:
             self.optimizer.step(self.grads)
