@@ -180,10 +180,12 @@ __device__ __forceinline__ f2 mul2_rn(f2 a, f2 b, f2 nz) { return fma2(a, b, nz)
 //   r = x - k ln2/64 with ln2/64 = C1 + C2 + C3: k C1 and k C2 are exact
 //     (11-bit constants, |k| < 2^13) and so are both subtractions, which
 //     leaves rh exact and rl = -k C3 (|rl| < 2^-22) as a correction;
-//   e^r - 1 = rh + rl (1 + rh) + rh^2 (1/2 + rh/6 + rh^2/24) + O(2^-44);
-//   2^(j/64) (j = k mod 64) as the float pair TH + TL from a 64-entry table;
-//   y = (TH + TL) e^r summed as s + ylo with an exact product TH rh and a
-//     Fast2Sum, then rounded.  If ylo +- 2^-37 round to the same float the
+//   2^(j/64) (j = k mod 64) = TH (1 + R) from a 64-entry table (TH the
+//     nearest float, R the float nearest to the remainder over TH);
+//   y = TH (1 + R) e^r = TH (1 + rh + tail) with
+//     tail = (rl + R)(1 + rh) + rh^2 (1/2 + rh/6 + rh^2/24) + O(2^-44),
+//     summed as s + ylo with an exact product TH rh and a Fast2Sum, then
+//     rounded.  If ylo +- 2^-37 round to the same float the
 //     exact value rounds to it too (rounding is monotonic and the error of
 //     s + ylo is below 2^-37 for y in [0.99, 2)), so that float is the
 //     correctly rounded result; it is scaled by 2^(k div 64) exactly.
@@ -222,7 +224,7 @@ static __device__ __noinline__ float expf_cr_slow(float x) {
   return __double2float_rn(y);
 }
 
-// The fast path on one element with its table entry T = 2^(j/64)
+// The fast path on one element with its table entry T = {TH, R}
 // (j = expf_cr_j(x)); *ok is false when the result must come from
 // expf_cr_slow.
 __device__ __forceinline__ uint32_t expf_cr_j(float x) {
@@ -233,16 +235,15 @@ __device__ __forceinline__ float expf_cr_fast(float x, float2 T, bool* ok) {
   const float kf = __fsub_rn(tk, kExpMagic);
   const float r1 = __fmaf_rn(kf, -kExpC1, x);
   const float rh = __fmaf_rn(kf, -kExpC2, r1);
-  const float rl = __fmul_rn(kf, -kExpC3);
-  const float w = __fmaf_rn(rl, rh, rl);
+  const float rlt = __fmaf_rn(kf, -kExpC3, T.y);  // rl + R
+  const float w = __fmaf_rn(rlt, rh, rlt);
   const float r2 = __fmul_rn(rh, rh);
   float p = __fmaf_rn(rh, kExpP4, kExpP3);
   p = __fmaf_rn(p, rh, 0.5f);
   const float tail = __fmaf_rn(r2, p, w);
   const float ph = __fmul_rn(T.x, rh), pl = __fmaf_rn(T.x, rh, -ph);
   const float s = __fadd_rn(T.x, ph), e1 = __fsub_rn(ph, __fsub_rn(s, T.x));
-  const float a = __fadd_rn(__fmaf_rn(T.x, tail, pl), e1);
-  const float ylo = __fadd_rn(a, __fmaf_rn(T.y, rh, T.y));
+  const float ylo = __fadd_rn(__fmaf_rn(T.x, tail, pl), e1);
   const float ra = __fadd_rn(s, __fadd_rn(ylo, kExpTie)), rb = __fadd_rn(s, __fsub_rn(ylo, kExpTie));
   *ok = ra == rb && fabsf(x) <= kExpFastMax;
   return __uint_as_float(__float_as_uint(ra) + ((__float_as_uint(tk) << 17) & 0xff800000u));
@@ -265,19 +266,18 @@ __device__ __forceinline__ f2 expf_cr2(f2 x, const float2* tab, f2 nz) {
   const f2 kf = sub2(tk, f2_dup(kExpMagic));
   const f2 r1 = fma2(kf, f2_dup(-kExpC1), x);
   const f2 rh = fma2(kf, f2_dup(-kExpC2), r1);
-  const f2 rl = mul2(kf, f2_dup(-kExpC3));
-  const f2 w = fma2(rl, rh, rl);
+  const uint32_t b0 = __float_as_uint(f2_lo(tk)), b1 = __float_as_uint(f2_hi(tk));
+  const float2 t0 = tab[b0 & 63u], t1 = tab[b1 & 63u];
+  const f2 th = f2_make(t0.x, t1.x), rel = f2_make(t0.y, t1.y);
+  const f2 rlt = fma2(kf, f2_dup(-kExpC3), rel);  // rl + R
+  const f2 w = fma2(rlt, rh, rlt);
   const f2 r2 = mul2(rh, rh);
   f2 p = fma2(rh, f2_dup(kExpP4), f2_dup(kExpP3));
   p = fma2(p, rh, f2_dup(0.5f));
   const f2 tail = fma2(r2, p, w);
-  const uint32_t b0 = __float_as_uint(f2_lo(tk)), b1 = __float_as_uint(f2_hi(tk));
-  const float2 t0 = tab[b0 & 63u], t1 = tab[b1 & 63u];
-  const f2 th = f2_make(t0.x, t1.x), tl = f2_make(t0.y, t1.y);
   const f2 ph = mul2_rn(th, rh, nz), pl = fma2(th, rh, neg2(ph));
   const f2 s = add2(th, ph), e1 = sub2(ph, sub2(s, th));
-  const f2 a = add2(fma2(th, tail, pl), e1);
-  const f2 ylo = add2(a, fma2(tl, rh, tl));
+  const f2 ylo = add2(fma2(th, tail, pl), e1);
   const f2 ra = add2(s, add2(ylo, f2_dup(kExpTie))), rb = add2(s, sub2(ylo, f2_dup(kExpTie)));
   float y0 = __uint_as_float(__float_as_uint(f2_lo(ra)) + ((b0 << 17) & 0xff800000u));
   float y1 = __uint_as_float(__float_as_uint(f2_hi(ra)) + ((b1 << 17) & 0xff800000u));

@@ -10,7 +10,9 @@ Every constant is derived here from ln 2 evaluated to 60 significant digits
   that k*C1 and k*C2 are exact floats for |k| < 2^13; C3 is the rest,
   rounded to float.
 * TH[j] + TL[j]: 2^(j/64) as an unevaluated sum of two floats (TH the
-  nearest float, TL the nearest float to the remainder).
+  nearest float, TL the nearest float to the remainder); the table stores
+  TH[j] and TL[j] / TH[j] (rounded to float), the low part relative to the
+  high one, so that it joins the reduction's correction term.
 * TD[j]: 2^(j/64) rounded to double; L1D + L2D: ln2/64 split for the
   double-precision path (L1D has 38 significant bits, so k*L1D is exact for
   |k| < 2^15).
@@ -53,15 +55,16 @@ def tables() -> dict:
     c1 = _bits(l64, 11)
     c2 = _bits(l64 - c1, 11)
     c3 = _f32(l64 - c1 - c2)
-    th, tl, td = [], [], []
+    th, tl, tlr, td = [], [], [], []
     for j in range(64):
         t = (Decimal(j) / 64 * LN2).exp()
         hi = _f32(t)
         th.append(hi)
         tl.append(_f32(t - Decimal(hi)))
+        tlr.append(_f32(Decimal(tl[-1]) / Decimal(hi)))
         td.append(float(t))  # float(Decimal) rounds to the nearest double
     l1d = _bits(l64, 38)
-    return dict(K64=_f32(Decimal(64) / LN2), C1=float(c1), C2=float(c2), C3=c3, TH=th, TL=tl, TD=td,
+    return dict(K64=_f32(Decimal(64) / LN2), C1=float(c1), C2=float(c2), C3=c3, TH=th, TL=tl, TLR=tlr, TD=td,
                 K64D=float(Decimal(64) / LN2), L1D=float(l1d), L2D=float(l64 - l1d))
 
 
@@ -70,16 +73,16 @@ def render(t: dict) -> str:
     lines = [
         "// exp_tables.cuh -- generated by gen_exp_tables.py; do not edit.",
         "// Constants of expf_cr (common.cuh): 64/ln2, ln2/64 in three parts,",
-        "// 2^(j/64) as float pairs and as doubles.",
+        "// 2^(j/64) as (float, relative float remainder) and as doubles.",
         "#pragma once",
         "namespace dsplat {",
         f"constexpr float kExpK64 = {fl(t['K64'])};",
         f"constexpr float kExpC1 = {fl(t['C1'])}, kExpC2 = {fl(t['C2'])}, kExpC3 = {fl(t['C3'])};",
         f"constexpr double kExpK64d = {t['K64D'].hex()}, kExpL1d = {t['L1D'].hex()}, kExpL2d = {t['L2D'].hex()};",
-        "// 2^(j/64) = hi + lo",
+        "// 2^(j/64) = hi (1 + rel): {hi, rel}",
         "static __device__ const float2 g_exp2_64[64] = {",
     ]
-    lines += [f"    {{{fl(h)}, {fl(l)}}}," for h, l in zip(t["TH"], t["TL"])]
+    lines += [f"    {{{fl(h)}, {fl(r)}}}," for h, r in zip(t["TH"], t["TLR"])]
     lines += ["};", "static __device__ const double g_exp2_64d[64] = {"]
     lines += [f"    {v.hex()}," for v in t["TD"]]
     lines += ["};", "}  // namespace dsplat", ""]
