@@ -78,11 +78,11 @@ struct Ent {  // one staged list entry (64 bytes), backward
 // 64-bit shared load yields the packed operand (96 bytes).  The conic is
 // kept as the reference reads it: (A, B, C) = (m0, m1, m2) with 2 m1 staged
 // (exact), px and m0 once (they enter through the per-lane column term).
-struct EntP {
-  float4 a;  // py, py, 2B, 2B
-  float4 b;  // C, C, opacity, opacity
+struct EntP {                // conic (A, B, C) staged times -1/2 (see make_entp)
+  float4 a;  // py, py, -B, -B
+  float4 b;  // -C/2, -C/2, opacity, opacity
   float4 c;  // r, r, g, g
-  float4 d;  // b, b, px, A
+  float4 d;  // b, b, px, -A/2
   float4 e;  // box x0, box x1, box y0, box y1
   float4 f;  // exponent in expf_cr's fast range (0/1 bits), list position (bits), -, -
   __device__ __forceinline__ void set_pos(uint32_t pos) { f.y = __uint_as_float(pos); }
@@ -95,13 +95,20 @@ __device__ __forceinline__ void make_entp(EntP* dst, float px, float py, float A
   // farthest corner; below 170 (rounding adds far less than the margin to
   // 174) every exponent -q/2 of the entry lies in expf_cr's fast range and
   // the per-pixel range check is skipped.  NaN or infinite terms fail it.
+  //
+  // The conic is staged times -1/2 (exact), so that the walk forms the
+  // exponent -q/2 directly: every product and sum of q scaled by -1/2 is the
+  // scaled rounding of the same operation on the unscaled values, except
+  // where an operand is subnormal -- and then |q| < 2^-100 and e^(-q/2)
+  // rounds to 1 either way.
   const float B2 = fa(B, B);
   const float dxm = fmaxf(fabsf(x0 - px), fabsf(x1 - px)), dym = fmaxf(fabsf(y0 - py), fabsf(y1 - py));
   const float mag = fabsf(A) * dxm * dxm + fabsf(B2) * dxm * dym + fabsf(C) * dym * dym;
-  dst->a = make_float4(py, py, B2, B2);
-  dst->b = make_float4(C, C, op, op);
+  const float hA = fm(A, -0.5f), hB2 = fm(B2, -0.5f), hC = fm(C, -0.5f);
+  dst->a = make_float4(py, py, hB2, hB2);
+  dst->b = make_float4(hC, hC, op, op);
   dst->c = make_float4(r, r, g, g);
-  dst->d = make_float4(b, b, px, A);
+  dst->d = make_float4(b, b, px, hA);
   dst->e = make_float4(x0, x1, y0, y1);
   dst->f = make_float4(__uint_as_float(mag < 170.f ? 1u : 0u), 0.f, 0.f, 0.f);
 }

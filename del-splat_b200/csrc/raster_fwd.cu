@@ -89,10 +89,10 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
         const float4 ed = sm[j].d;                                             // b, b, px, A
         const f2 qbl = f2_make(ed.x, ed.y);
         const float2 ef = *reinterpret_cast<const float2*>(&sm[j].f);
-        // q = A dx dx + B (dx dy + dy dx) + C dy dy in the reference's
-        // order (mat2_sym::mult_vec_from_both_sides); dx is fixed per lane,
-        // so (A dx) dx is formed once per entry, and B (dx dy + dy dx) is
-        // (2B)(dx dy) exactly
+        // -q/2 with q = A dx dx + B (dx dy + dy dx) + C dy dy in the
+        // reference's order (mat2_sym::mult_vec_from_both_sides), from the
+        // conic staged times -1/2; dx is fixed per lane, so (A dx) dx is
+        // formed once per entry, and B (dx dy + dy dx) is (2B)(dx dy) exactly
         const float dx = fs(fx, ed.z);
         const f2 adxdx2 = f2_dup(__fmaf_rn(fm(ed.w, dx), dx, nz));
         const f2 dx2 = f2_dup(dx);
@@ -112,7 +112,7 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
             const f2 dy2 = sub2(fy2[q], qa.x);
             const f2 qf = add2(add2(adxdx2, mul2_rn(qa.y, mul2(dx2, dy2), nz2)),
                                mul2_rn(mul2(qb.x, dy2), dy2, nz2));
-            const f2 g2 = expf_cr2<!decltype(inrange)::value>(mul2(qf, f2_dup(-0.5f)), tab, nz2);
+            const f2 g2 = expf_cr2<!decltype(inrange)::value>(qf, tab, nz2);
             const f2 al = mul2_rn(g2, qb.y, nz2);
             // an inactive slot of the pair takes alpha 0: its state is unchanged
             const f2 e2 = f2_make(a0 ? f2_lo(al) : 0.f, a1 ? f2_hi(al) : 0.f);
