@@ -168,10 +168,11 @@ KERNEL_OF_STAGE = {"raster_fwd": "k_raster_fwd", "raster_bwd": "k_raster_bwd", "
 
 def captured_figures(stage: str, workload: str):
     """Per-launch figures of a stage's kernel from the committed ncu summary
-    of this very build: lines `capture_build <hash>`, `workload <text>` and
-    `per_launch <workload> <kernel> inst <warp-instructions> dram_bytes
-    <bytes>` in a profiles/*.md.  None when no capture of the current sources
-    exists (the line then says so instead of reporting a stale figure)."""
+    of this very build: lines `capture_build <hash>`, `workload <workload>:
+    <description>` and `per_launch <workload> <kernel> inst
+    <warp-instructions> dram_bytes <bytes>` in a profiles/*.md.  None when
+    no capture of the current sources exists (the line then says so instead
+    of reporting a stale figure)."""
     import glob
     import re
     kernel = KERNEL_OF_STAGE.get(stage)
@@ -184,7 +185,7 @@ def captured_figures(stage: str, workload: str):
         m_build = re.search(r"capture_build\s+([0-9a-f]+)", txt)
         m = re.search(r"per_launch\s+" + workload + r"\s+" + kernel + r"\s+inst\s+(\d+)\s+dram_bytes\s+(\d+)", txt)
         if m and m_build and m_build.group(1) == want:
-            wl = re.search(r"workload\s+(.+)", txt)
+            wl = re.search(r"^\s*workload\s+" + workload + r":\s*(.+)$", txt, re.M)
             return {"inst": int(m.group(1)), "dram_bytes": int(m.group(2)),
                     "capture": os.path.relpath(path, ROOT), "workload": wl.group(1).strip() if wl else None}
     return None
