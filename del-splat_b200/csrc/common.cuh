@@ -157,8 +157,6 @@ __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
   return r;
 }
 
-__device__ __forceinline__ f2 neg2(f2 a) { return a ^ 0x8000000080000000ull; }
-
 // A packed product that keeps its own rounding when it feeds an add.  The
 // assembler fuses a mul.rn.f32x2 whose result goes into an add.rn.f32x2 into
 // one fused multiply-add (a single rounding) -- with or without -fmad=false,
@@ -184,11 +182,14 @@ __device__ __forceinline__ f2 mul2_rn(f2 a, f2 b, f2 nz) { return fma2(a, b, nz)
 //     nearest float, R the float nearest to the remainder over TH);
 //   y = TH (1 + R) e^r = TH (1 + rh + tail) with
 //     tail = (rl + R)(1 + rh) + rh^2 (1/2 + rh/6 + rh^2/24) + O(2^-44),
-//     summed as s + ylo with an exact product TH rh and a Fast2Sum, then
-//     rounded.  If ylo +- 2^-37 round to the same float the
-//     exact value rounds to it too (rounding is monotonic and the error of
-//     s + ylo is below 2^-37 for y in [0.99, 2)), so that float is the
-//     correctly rounded result; it is scaled by 2^(k div 64) exactly.
+//     evaluated as rh (rh p + (rl + R)) + (rl + R);
+//   s = RN(TH + TH rh) by one fma, its rounding error TH rh + (TH - s)
+//     (TH - s is exact: s and TH are within a factor 2) by a second fma,
+//     ylo = TH tail + that error by a third: y = s + ylo.  If ylo +- 2^-37
+//     round to the same float with s, the exact value rounds to it too
+//     (rounding is monotonic and the error of s + ylo is below 2^-37 for y
+//     in [0.99, 2)), so that float is the correctly rounded result; it is
+//     scaled by 2^(k div 64) exactly.
 // Otherwise (|x| > 87, NaN, or the rounding test failed -- about 4e-5 of
 // the inputs), expf_cr_slow evaluates the same reduction in double precision
 // (degree-6 polynomial, 2^(j/64) rounded to double) and rounds the double
@@ -224,64 +225,67 @@ static __device__ __noinline__ float expf_cr_slow(float x) {
   return __double2float_rn(y);
 }
 
-// The fast path on one element with its table entry T = {TH, R}
-// (j = expf_cr_j(x)); *ok is false when the result must come from
-// expf_cr_slow.
-__device__ __forceinline__ uint32_t expf_cr_j(float x) {
-  return __float_as_uint(__fmaf_rn(x, kExpK64, kExpMagic)) & 63u;
+// The fast path's arithmetic, written once for one element (V = float) and
+// for two (V = f2, packed): each packed operation rounds each element
+// exactly as the scalar one, so both forms give the same bits.  Every
+// product feeds an explicit fma, so no contraction can change a rounding.
+__device__ __forceinline__ float vfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float vadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float vsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ f2 vfma(f2 a, f2 b, f2 c) { return fma2(a, b, c); }
+__device__ __forceinline__ f2 vadd(f2 a, f2 b) { return add2(a, b); }
+__device__ __forceinline__ f2 vsub(f2 a, f2 b) { return sub2(a, b); }
+template <class V> __device__ __forceinline__ V vdup(float a);
+template <> __device__ __forceinline__ float vdup<float>(float a) { return a; }
+template <> __device__ __forceinline__ f2 vdup<f2>(float a) { return f2_dup(a); }
+
+// tk = x 64/ln2 + 1.5 2^23: its low bits hold k (table index k & 63)
+template <class V>
+__device__ __forceinline__ V expf_cr_tk(V x) {
+  return vfma(x, vdup<V>(kExpK64), vdup<V>(kExpMagic));
 }
-__device__ __forceinline__ float expf_cr_fast(float x, float2 T, bool* ok) {
-  const float tk = __fmaf_rn(x, kExpK64, kExpMagic);
-  const float kf = __fsub_rn(tk, kExpMagic);
-  const float r1 = __fmaf_rn(kf, -kExpC1, x);
-  const float rh = __fmaf_rn(kf, -kExpC2, r1);
-  const float rlt = __fmaf_rn(kf, -kExpC3, T.y);  // rl + R
-  const float w = __fmaf_rn(rlt, rh, rlt);
-  const float r2 = __fmul_rn(rh, rh);
-  float p = __fmaf_rn(rh, kExpP4, kExpP3);
-  p = __fmaf_rn(p, rh, 0.5f);
-  const float tail = __fmaf_rn(r2, p, w);
-  const float ph = __fmul_rn(T.x, rh), pl = __fmaf_rn(T.x, rh, -ph);
-  const float s = __fadd_rn(T.x, ph), e1 = __fsub_rn(ph, __fsub_rn(s, T.x));
-  const float ylo = __fadd_rn(__fmaf_rn(T.x, tail, pl), e1);
-  const float ra = __fadd_rn(s, __fadd_rn(ylo, kExpTie)), rb = __fadd_rn(s, __fsub_rn(ylo, kExpTie));
-  *ok = ra == rb && fabsf(x) <= kExpFastMax;
+// ra, rb: s + ylo rounded with ylo moved by +-2^-37 (equal: the fast path
+// holds), before the scaling by 2^(k div 64); th, rel = the table entry
+template <class V>
+__device__ __forceinline__ void expf_cr_round(V x, V tk, V th, V rel, V* ra, V* rb) {
+  const V kf = vsub(tk, vdup<V>(kExpMagic));
+  const V r1 = vfma(kf, vdup<V>(-kExpC1), x);
+  const V rh = vfma(kf, vdup<V>(-kExpC2), r1);
+  const V rlt = vfma(kf, vdup<V>(-kExpC3), rel);  // rl + R
+  V p = vfma(rh, vdup<V>(kExpP4), vdup<V>(kExpP3));
+  p = vfma(p, rh, vdup<V>(0.5f));
+  const V tail = vfma(rh, vfma(rh, p, rlt), rlt);
+  const V s = vfma(th, rh, th);
+  const V ylo = vfma(th, tail, vfma(th, rh, vsub(th, s)));
+  *ra = vadd(s, vadd(ylo, vdup<V>(kExpTie)));
+  *rb = vadd(s, vsub(ylo, vdup<V>(kExpTie)));
+}
+// ra scaled by 2^(k div 64) (exact: no subnormal result for |x| <= 87)
+__device__ __forceinline__ float expf_cr_scale(float ra, float tk) {
   return __uint_as_float(__float_as_uint(ra) + ((__float_as_uint(tk) << 17) & 0xff800000u));
 }
 
 // Scalar form, table read from global memory.
 __device__ __forceinline__ float expf_cr(float x) {
-  bool ok;
-  const float y = expf_cr_fast(x, __ldg(&g_exp2_64[expf_cr_j(x)]), &ok);
-  return ok ? y : expf_cr_slow(x);
+  const float tk = expf_cr_tk(x);
+  const float2 t = __ldg(&g_exp2_64[__float_as_uint(tk) & 63u]);
+  float ra, rb;
+  expf_cr_round(x, tk, t.x, t.y, &ra, &rb);
+  return ra == rb && fabsf(x) <= kExpFastMax ? expf_cr_scale(ra, tk) : expf_cr_slow(x);
 }
 
 // Packed form for two elements, table in shared memory (tab: a copy of
 // g_exp2_64).  RANGE: check |x| <= 87 per element (a caller that has bounded
-// x for a whole batch passes false).  nz: (-0, -0) held in a runtime value
-// (see mul2_rn).  Each element equals expf_cr of it.
+// x for a whole batch passes false).  Each element equals expf_cr of it.
 template <bool RANGE>
-__device__ __forceinline__ f2 expf_cr2(f2 x, const float2* tab, f2 nz) {
-  const f2 tk = fma2(x, f2_dup(kExpK64), f2_dup(kExpMagic));
-  const f2 kf = sub2(tk, f2_dup(kExpMagic));
-  const f2 r1 = fma2(kf, f2_dup(-kExpC1), x);
-  const f2 rh = fma2(kf, f2_dup(-kExpC2), r1);
-  const uint32_t b0 = __float_as_uint(f2_lo(tk)), b1 = __float_as_uint(f2_hi(tk));
-  const float2 t0 = tab[b0 & 63u], t1 = tab[b1 & 63u];
-  const f2 th = f2_make(t0.x, t1.x), rel = f2_make(t0.y, t1.y);
-  const f2 rlt = fma2(kf, f2_dup(-kExpC3), rel);  // rl + R
-  const f2 w = fma2(rlt, rh, rlt);
-  const f2 r2 = mul2(rh, rh);
-  f2 p = fma2(rh, f2_dup(kExpP4), f2_dup(kExpP3));
-  p = fma2(p, rh, f2_dup(0.5f));
-  const f2 tail = fma2(r2, p, w);
-  const f2 ph = mul2_rn(th, rh, nz), pl = fma2(th, rh, neg2(ph));
-  const f2 s = add2(th, ph), e1 = sub2(ph, sub2(s, th));
-  const f2 ylo = add2(fma2(th, tail, pl), e1);
-  const f2 ra = add2(s, add2(ylo, f2_dup(kExpTie))), rb = add2(s, sub2(ylo, f2_dup(kExpTie)));
-  float y0 = __uint_as_float(__float_as_uint(f2_lo(ra)) + ((b0 << 17) & 0xff800000u));
-  float y1 = __uint_as_float(__float_as_uint(f2_hi(ra)) + ((b1 << 17) & 0xff800000u));
-  bool ok = ra == rb;
+__device__ __forceinline__ f2 expf_cr2(f2 x, const float2* tab) {
+  const f2 tk = expf_cr_tk(x);
+  const float k0 = f2_lo(tk), k1 = f2_hi(tk);
+  const float2 t0 = tab[__float_as_uint(k0) & 63u], t1 = tab[__float_as_uint(k1) & 63u];
+  f2 ra, rb;
+  expf_cr_round(x, tk, f2_make(t0.x, t1.x), f2_make(t0.y, t1.y), &ra, &rb);
+  float y0 = expf_cr_scale(f2_lo(ra), k0), y1 = expf_cr_scale(f2_hi(ra), k1);
+  bool ok = ra == rb;  // both elements (64-bit compare; no zero or NaN in range)
   if (RANGE) ok = ok && fabsf(f2_lo(x)) <= kExpFastMax && fabsf(f2_hi(x)) <= kExpFastMax;
   if (!ok) {  // rare: settle each element on its own
     if (!(f2_lo(ra) == f2_lo(rb) && fabsf(f2_lo(x)) <= kExpFastMax)) y0 = expf_cr_slow(f2_lo(x));

@@ -384,7 +384,7 @@ __global__ void k_adam(size_t n, float* __restrict__ p, const float* __restrict_
 
 // Fused Adam over the five parameter tensors of a Gaussian scene (one
 // launch), with the step count kept on the device so that a captured graph
-// replays correctly: every thread reads t = *step + 1 and k_adam_step_inc
+// replays correctly: every block reads t = *step + 1 and k_adam_step_inc
 // stores it after the update.  The update is torch.optim.Adam's (no weight
 // decay, no amsgrad), in its order: m += (1-b1)(g - m); v = v b2 + (1-b2) g^2;
 // p -= (lr / (1 - b1^t)) m / (sqrt(v) / sqrt(1 - b2^t) + eps), with the
@@ -394,27 +394,76 @@ __global__ void k_adam(size_t n, float* __restrict__ p, const float* __restrict_
 // front of an entry as T / (1 - alpha)).
 constexpr float kOpacityMax = 0.999f;
 
-__global__ void k_adam_fused(AdamSeg seg, double lr, double b1, double b2, double eps,
-                             const int32_t* __restrict__ step) {
-  const size_t total = seg.end[4];
-  const double t = double(*step + 1);
-  const float step_size = float(lr / (1.0 - pow(b1, t)));
-  const float bc2_sqrt = float(sqrt(1.0 - pow(b2, t)));
+// One Adam element update (the order above); CLAMP keeps the result in
+// [0, kOpacityMax].
+template <bool CLAMP>
+__device__ __forceinline__ void adam_elem(float& p, float g, float& m, float& v, float step_size, float bc2_sqrt,
+                                          float w1, float b2f, float w2, float epsf) {
+  m = m + w1 * (g - m);
+  v = v * b2f + w2 * (g * g);
+  const float denom = sqrtf(v) / bc2_sqrt + epsf;
+  p = p - step_size * (m / denom);
+  if (CLAMP) p = fminf(fmaxf(p, 0.f), kOpacityMax);
+}
+
+// One tensor of the scene: 16-byte vectors when its four arrays allow them
+// (the same element operations), the rest element by element.
+template <bool CLAMP>
+__device__ __forceinline__ void adam_tensor(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                                            float* __restrict__ v, size_t n, float step_size, float bc2_sqrt,
+                                            float w1, float b2f, float w2, float epsf) {
+  const size_t tid = size_t(blockIdx.x) * blockDim.x + threadIdx.x, stride = size_t(gridDim.x) * blockDim.x;
+  size_t head = 0;
+  const bool vec = ((reinterpret_cast<uintptr_t>(p) | reinterpret_cast<uintptr_t>(g) |
+                     reinterpret_cast<uintptr_t>(m) | reinterpret_cast<uintptr_t>(v)) & 15u) == 0;
+  if (vec) {
+    const size_t n4 = n / 4;
+    float4* p4 = reinterpret_cast<float4*>(p);
+    const float4* g4 = reinterpret_cast<const float4*>(g);
+    float4* m4 = reinterpret_cast<float4*>(m);
+    float4* v4 = reinterpret_cast<float4*>(v);
+    for (size_t i = tid; i < n4; i += stride) {
+      float4 pp = p4[i], mm = m4[i], vv = v4[i];
+      const float4 gg = __ldg(g4 + i);
+      adam_elem<CLAMP>(pp.x, gg.x, mm.x, vv.x, step_size, bc2_sqrt, w1, b2f, w2, epsf);
+      adam_elem<CLAMP>(pp.y, gg.y, mm.y, vv.y, step_size, bc2_sqrt, w1, b2f, w2, epsf);
+      adam_elem<CLAMP>(pp.z, gg.z, mm.z, vv.z, step_size, bc2_sqrt, w1, b2f, w2, epsf);
+      adam_elem<CLAMP>(pp.w, gg.w, mm.w, vv.w, step_size, bc2_sqrt, w1, b2f, w2, epsf);
+      p4[i] = pp;
+      m4[i] = mm;
+      v4[i] = vv;
+    }
+    head = n4 * 4;
+  }
+  for (size_t i = head + tid; i < n; i += stride) {
+    float pp = p[i], mm = m[i], vv = v[i];
+    adam_elem<CLAMP>(pp, g[i], mm, vv, step_size, bc2_sqrt, w1, b2f, w2, epsf);
+    p[i] = pp;
+    m[i] = mm;
+    v[i] = vv;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_adam_fused(AdamSeg seg, double lr, double b1, double b2, double eps,
+                                                    const int32_t* __restrict__ step) {
+  __shared__ float coef[2];
+  if (threadIdx.x == 0) {  // bias corrections once per block
+    const double t = double(*step + 1);
+    coef[0] = float(lr / (1.0 - pow(b1, t)));
+    coef[1] = float(sqrt(1.0 - pow(b2, t)));
+  }
+  __syncthreads();
+  const float step_size = coef[0], bc2_sqrt = coef[1];
   const float w1 = float(1.0 - b1), b2f = float(b2), w2 = float(1.0 - b2), epsf = float(eps);
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
-    int k = 0;
+  size_t begin = 0;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) k += i >= seg.end[j];
-    const size_t o = i - (k ? seg.end[k - 1] : 0);
-    const float gi = seg.g[k][o];
-    const float mi = seg.m[k][o] + w1 * (gi - seg.m[k][o]);
-    const float vi = seg.v[k][o] * b2f + w2 * (gi * gi);
-    seg.m[k][o] = mi;
-    seg.v[k][o] = vi;
-    const float denom = sqrtf(vi) / bc2_sqrt + epsf;
-    float pi = seg.p[k][o] - step_size * (mi / denom);
-    if (k == 3) pi = fminf(fmaxf(pi, 0.f), kOpacityMax);
-    seg.p[k][o] = pi;
+  for (int k = 0; k < 5; ++k) {
+    const size_t n = seg.end[k] - begin;
+    if (k == 3)
+      adam_tensor<true>(seg.p[k], seg.g[k], seg.m[k], seg.v[k], n, step_size, bc2_sqrt, w1, b2f, w2, epsf);
+    else
+      adam_tensor<false>(seg.p[k], seg.g[k], seg.m[k], seg.v[k], n, step_size, bc2_sqrt, w1, b2f, w2, epsf);
+    begin = seg.end[k];
   }
 }
 

@@ -112,7 +112,7 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
             const f2 dy2 = sub2(fy2[q], qa.x);
             const f2 qf = add2(add2(adxdx2, mul2_rn(qa.y, mul2(dx2, dy2), nz2)),
                                mul2_rn(mul2(qb.x, dy2), dy2, nz2));
-            const f2 g2 = expf_cr2<!decltype(inrange)::value>(qf, tab, nz2);
+            const f2 g2 = expf_cr2<!decltype(inrange)::value>(qf, tab);
             const f2 al = mul2_rn(g2, qb.y, nz2);
             // an inactive slot of the pair takes alpha 0: its state is unchanged
             const f2 e2 = f2_make(a0 ? f2_lo(al) : 0.f, a1 ? f2_hi(al) : 0.f);
