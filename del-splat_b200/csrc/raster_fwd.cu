@@ -19,7 +19,13 @@ namespace dsplat {
 // ---------------------------------------------------------------------------
 // CUDA_STOP: the stop test of the reference's CUDA kernel (alpha_sum >=
 // 0.999f, its double comparison) instead of del-splat-cpu's (> 0.999f).
-template <int TS, int PPL_, bool CUDA_STOP, class Walk, class Src>
+// SPLIT (a 16x8 task of two 8x8 tiles, 4 slots per lane): lane L covers
+// column L % 8 of both tiles at rows L / 8 and L / 8 + 4, slot pair 0 in the
+// left tile and pair 1 in the right one, so that an entry whose box meets
+// one tile keeps every lane of the warp busy on one pair and skips the
+// other pair warp-wide.  Otherwise lane L covers column L % TS, slot k at
+// row L / TS + k (32 / TS).
+template <int TS, int PPL_, bool CUDA_STOP, bool SPLIT, class Walk, class Src>
 __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, EntP* sm, const float2* tab, float nz,
                                          uint32_t s, uint32_t e, int px0, int py0, int w, int h, int xend, bool accumulate,
                                          float* __restrict__ out_rgb, size_t pix_base, float* __restrict__ out_T,
@@ -29,16 +35,22 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
   constexpr int PPL = G::PPL;
   static_assert(PPL % 2 == 0, "pixel slots are evaluated in pairs");
   constexpr int NP = PPL / 2;
+  static_assert(!SPLIT || (TS == 16 && PPL == 4), "split lanes: two 8-wide tiles, two slot pairs");
+  constexpr int COLS = SPLIT ? TS / 2 : TS;
+  constexpr int RSTEP = SPLIT ? 4 : G::ROW_STEP;
   const int lane = threadIdx.x & 31;
-  const int ix = px0 + (lane % TS);
-  const int iy0 = py0 + (lane / TS);
-  const float fx = float(ix) + 0.5f;
+  const int col = lane % COLS, row0 = lane / COLS;
+  auto slot_x = [&](int k) { return px0 + col + (SPLIT ? (k / 2) * COLS : 0); };
+  auto slot_y = [&](int k) { return py0 + row0 + (SPLIT ? k % 2 : k) * RSTEP; };
+  float fxp[NP];  // column centre of each slot pair
+#pragma unroll
+  for (int q = 0; q < NP; ++q) fxp[q] = float(slot_x(2 * q)) + 0.5f;
   float T[PPL], as[PPL], c0[PPL], c1[PPL], c2[PPL], fy[PPL];
   uint32_t last[PPL];
   uint32_t live = 0;
 #pragma unroll
   for (int k = 0; k < PPL; ++k) {
-    const int iy = iy0 + k * G::ROW_STEP;
+    const int ix = slot_x(k), iy = slot_y(k);
     fy[k] = float(iy) + 0.5f;
     T[k] = 1.f;
     as[k] = 0.f;
@@ -82,7 +94,10 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
     if (live) {
       for (int j = 0; j < k_staged; ++j) {
         const float4 ee = sm[j].e;
-        if (!(ee.x <= fx && fx <= ee.y)) continue;
+        // column tests: the slot pairs' columns (one column unless SPLIT)
+        const bool cin0 = ee.x <= fxp[0] && fxp[0] <= ee.y;
+        const bool cin1 = SPLIT ? (ee.x <= fxp[NP - 1] && fxp[NP - 1] <= ee.y) : cin0;
+        if (!(cin0 || cin1)) continue;
         const ulonglong2 qa = *reinterpret_cast<const ulonglong2*>(&sm[j].a);  // (py,py) (2B,2B)
         const ulonglong2 qb = *reinterpret_cast<const ulonglong2*>(&sm[j].b);  // (C,C) (op,op)
         const ulonglong2 qc = *reinterpret_cast<const ulonglong2*>(&sm[j].c);  // (r,r) (g,g)
@@ -91,11 +106,16 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
         const float2 ef = *reinterpret_cast<const float2*>(&sm[j].f);
         // -q/2 with q = A dx dx + B (dx dy + dy dx) + C dy dy in the
         // reference's order (mat2_sym::mult_vec_from_both_sides), from the
-        // conic staged times -1/2; dx is fixed per lane, so (A dx) dx is
-        // formed once per entry, and B (dx dy + dy dx) is (2B)(dx dy) exactly
-        const float dx = fs(fx, ed.z);
-        const f2 adxdx2 = f2_dup(__fmaf_rn(fm(ed.w, dx), dx, nz));
-        const f2 dx2 = f2_dup(dx);
+        // conic staged times -1/2; dx is fixed per slot pair, so (A dx) dx
+        // is formed once per entry and column, and B (dx dy + dy dx) is
+        // (2B)(dx dy) exactly
+        auto col_terms = [&](float fxq, f2* adxdx2, f2* dx2) {
+          const float dx = fs(fxq, ed.z);
+          *adxdx2 = f2_dup(__fmaf_rn(fm(ed.w, dx), dx, nz));
+          *dx2 = f2_dup(dx);
+        };
+        f2 adxdx2_1 = 0, dx2_1 = 0;  // the lane's column (all pairs) unless SPLIT
+        if (!SPLIT) col_terms(fxp[0], &adxdx2_1, &dx2_1);
         const uint32_t pos = __float_as_uint(ef.y);
         // all instances compute the same bits: `inrange` skips expf_cr's
         // range check (proven by the entry's staged flag), `rows` the row
@@ -106,9 +126,12 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
             // a slot is one row of the slab across the warp: the skips are
             // warp-uniform in practice
             const int k0 = 2 * q, k1 = 2 * q + 1;
+            if (SPLIT && !(q == 0 ? cin0 : cin1)) continue;
             const bool a0 = ((live >> k0) & 1u) && (decltype(rows)::value || (ee.z <= fy[k0] && fy[k0] <= ee.w));
             const bool a1 = ((live >> k1) & 1u) && (decltype(rows)::value || (ee.z <= fy[k1] && fy[k1] <= ee.w));
             if (!(a0 || a1)) continue;
+            f2 adxdx2 = adxdx2_1, dx2 = dx2_1;
+            if (SPLIT) col_terms(fxp[q], &adxdx2, &dx2);
             const f2 dy2 = sub2(fy2[q], qa.x);
             const f2 qf = add2(add2(adxdx2, mul2_rn(qa.y, mul2(dx2, dy2), nz2)),
                                mul2_rn(mul2(qb.x, dy2), dy2, nz2));
@@ -166,8 +189,7 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
 #pragma unroll
   for (int k = 0; k < PPL; ++k) {
     if (!((inside >> k) & 1u)) continue;
-    const int iy = iy0 + k * G::ROW_STEP;
-    const size_t p = pix_base + size_t(iy) * w + ix;
+    const size_t p = pix_base + size_t(slot_y(k)) * w + slot_x(k);
     out_rgb[3 * p] = c0[k];
     out_rgb[3 * p + 1] = c1[k];
     out_rgb[3 * p + 2] = c2[k];
@@ -228,7 +250,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     PackedSrc src{rec + 3 * size_t(ig.v) * n};
     SbWalkSpan walk{list1, ig.lx, ig.ly, nx};
     const int xend = min(vd.w, ig.px0 + int(nx) * TS);
-    const uint32_t walked = fwd_slab<G::GX, G::PPL, false>(
+    const uint32_t walked = fwd_slab<G::GX, G::PPL, false, NT == 2 && G::PPL == 4>(
         walk, src, sm, tab, nz, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, xend, false, out_rgb,
         vd.pix_base, out_T, out_last, target, grad_pix, slab_loss ? slab_loss + size_t(item) * G::SLABS + slab : nullptr);
     // scheduling hint for the backward and the next forward: list positions walked
@@ -255,7 +277,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
   const int px0 = int(tile % uint32_t(tile_w)) * TS;
   const int py0 = int(tile / uint32_t(tile_w)) * TS + int(slab) * G::SLAB_ROWS;
   TileWalk walk{idx2pnt};
-  fwd_slab<TS, PPL, CUDA_STOP>(walk, src, sm, tab, nz, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, w, true, pix2rgb, 0, out_T,
+  fwd_slab<TS, PPL, CUDA_STOP, false>(walk, src, sm, tab, nz, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, w, true, pix2rgb, 0, out_T,
                     out_last, nullptr, nullptr, nullptr);
 }
 
