@@ -487,6 +487,50 @@ STAGE_NAMES = ["project_fwd", "depth_sort", "sb_lists", "task_order", "raster_fw
                "raster_bwd", "project_bwd"]
 
 
+def time_dropin(base, cams, dev, steps: int, warmup: int, world: int) -> dict:
+    """Forward only, one view per call, through the reference-shaped chain a
+    del-splat-cudarc caller runs (splat_gauss.rs:6-195): the drop-in
+    projection, tile2idx_idx2pnt (the count with its device-to-host read of
+    the pair total, then the fill into buffers allocated per call, as the
+    reference allocates them) and rasterize_pnt2splat2 at the reference's
+    16x16 tiles.  That chain takes per-point RGB (the reference has no SH), so
+    the SH DC colours stand in.  Beside it, the batched forward of the same
+    views (SH 3) with the same event timing."""
+    from dsplat import cudarc
+    n = base.n
+    means = torch.from_numpy(np.ascontiguousarray(base.means)).to(dev)
+    scales = torch.from_numpy(np.ascontiguousarray(base.scales)).to(dev)
+    quats = torch.from_numpy(np.ascontiguousarray(base.quats)).to(dev)
+    opacity = torch.from_numpy(np.ascontiguousarray(base.opacity)).to(dev)
+    rgb = torch.from_numpy(np.ascontiguousarray(base.colors.reshape(n, -1, 3)[:, 0, :])).to(dev)
+    xyd, conic, aabb = (torch.empty((n, k), device=dev) for k in (3, 3, 4))
+    mvps = [torch.from_numpy(np.ascontiguousarray(c.mvp)).to(dev) for c in cams]
+    imgs = [torch.zeros((c.height, c.width, 3), device=dev) for c in cams]
+
+    def step():
+        for c, mvp, img in zip(cams, mvps, imgs):
+            size = (c.width, c.height)
+            cudarc.splat_gauss_pnt2splat3_to_pnt2splat2(None, means, scales, quats, xyd, conic, aabb, mvp, size)
+            t2i, i2p = cudarc.splat_gauss_tile2idx_idx2pnt(None, size, 16, xyd, aabb)
+            img.zero_()
+            cudarc.splat_gauss_rasterize_pnt2splat2(None, size, img, xyd, conic, aabb, opacity, rgb, 16, t2i, i2p)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    t = max_over_ranks(e0.elapsed_time(e1), world, dev)
+    return {"views_per_s": world * len(cams) * steps / (t / 1e3), "ms_per_16_views": t / steps,
+            "chain": "pnt2splat3_to_pnt2splat2 -> tile2idx_idx2pnt (count: D2H sync; fill: per-call buffers) "
+                     "-> rasterize_pnt2splat2, 16x16 tiles, one view per call, forward only, SH DC as RGB"}
+
+
 def measure_stages(L, step, steps: int) -> np.ndarray:
     """Mean per-stage times (ms, CUDA events recorded on the launch stream by
     the library's stage hook) of `steps` eager runs of step()."""
@@ -671,6 +715,7 @@ def main():
     ap.add_argument("--no-graph", action="store_true", help="time the batched step without CUDA-graph replay")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-dropin", action="store_true", help="skip the forward-only drop-in chain leg")
     ap.add_argument("--workload", default="gauss-batch", choices=["gauss-batch", "zbuffer", "train4m"],
                     help="gauss-batch: the headline (default); zbuffer: 1M-point circle z-buffer at 1024x1024; "
                          "train4m: 4M Gaussians, 8 views at 1080p, fwd+bwd+Adam")
@@ -813,6 +858,26 @@ def main():
         parity[f"batched_vs_plain_max_abs_ts{cfg[0]}_ppl{cfg[1]}"] = worst
     plain_cfgs = plain = None  # release the per-view workspaces
 
+    # forward only: the reference-shaped drop-in chain one view per call,
+    # beside the batched forward of the same views
+    fwd_only = None
+    if not args.no_dropin:
+        fwd_only = {"dropin": time_dropin(base, cams, dev, args.steps, args.warmup, world)}
+        for _ in range(args.warmup):
+            batch.forward(params)
+        torch.cuda.synchronize()
+        barrier(world)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for _ in range(args.steps):
+            batch.forward(params)
+        f1.record()
+        torch.cuda.synchronize()
+        ft = max_over_ranks(f0.elapsed_time(f1), world, dev)
+        fwd_only["batched"] = {"views_per_s": world * V * args.steps / (ft / 1e3), "ms_per_16_views": ft / args.steps,
+                               "chain": "dsplat_gauss_batch_forward, eager, SH 3"}
+        fwd_only["batched_over_dropin"] = fwd_only["batched"]["views_per_s"] / fwd_only["dropin"]["views_per_s"]
+
     # end to end through the public API: every step's inputs (parameters and
     # targets) come from pinned host memory and every step's result -- the
     # rendered images of all views and the loss -- goes back to pinned host
@@ -916,6 +981,7 @@ def main():
                        if plain_cfg else None,
                        "plain_views_per_s_by_config": plain_by_cfg or None,
                        "batched_over_plain": (value / world) / (plain_vps / world) if plain_vps else None,
+                       "forward_only": fwd_only,
                        "l2": "inputs larger than L2 (params 236 MB, pair lists > 1 GB)",
                        "parallelism": f"replicas x{world} (views sharded, no collective)",
                        "stage_ms": {n: round(float(stage_ms[i]), 4) for i, n in enumerate(names)}},

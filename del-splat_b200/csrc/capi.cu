@@ -658,9 +658,11 @@ int dsplat_circle_splat_zbuffer(dsplat_stream stream, uint32_t num_pnt, const fl
     return fail(DSPLAT_ERR_INVALID_ARG, "null pointer");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   k_fill_u64<<<blocks_for(npix, 256), 256, 0, st>>>(zbuf, npix, ~0ull); count_launch();
-  if (num_pnt > 0)
+  if (num_pnt > 0) {
     k_circle_zbuf<<<blocks_for(num_pnt, 128), 128, 0, st>>>(num_pnt, pnt2pixxydepth, pnt2pixrad, int(img_w),
-                                                           int(img_h), int(tile_size), zbuf); count_launch();
+                                                           int(img_h), int(tile_size), zbuf);
+    count_launch();
+  }
   k_circle_resolve<<<blocks_for(npix, 256), 256, 0, st>>>(npix, zbuf, colors, color_kind, pix, pix2winner); count_launch();
   TRY_CUDA(cudaGetLastError(), "circle zbuffer");
   return DSPLAT_OK;
