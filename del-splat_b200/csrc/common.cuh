@@ -274,16 +274,18 @@ __device__ __forceinline__ float expf_cr(float x) {
   return ra == rb && fabsf(x) <= kExpFastMax ? expf_cr_scale(ra, tk) : expf_cr_slow(x);
 }
 
-// Packed form for two elements, table in shared memory (tab: a copy of
-// g_exp2_64).  RANGE: check |x| <= 87 per element (a caller that has bounded
-// x for a whole batch passes false).  Each element equals expf_cr of it.
+// Packed form for two elements, table in shared memory (tab: g_exp2_64 as
+// two planes, tab[j] = hi and tab[64 + j] = rel, so that each element's
+// value loads straight into its half of the packed operand).  RANGE: check
+// |x| <= 87 per element (a caller that has bounded x for a whole batch
+// passes false).  Each element equals expf_cr of it.
 template <bool RANGE>
-__device__ __forceinline__ f2 expf_cr2(f2 x, const float2* tab) {
+__device__ __forceinline__ f2 expf_cr2(f2 x, const float* tab) {
   const f2 tk = expf_cr_tk(x);
   const float k0 = f2_lo(tk), k1 = f2_hi(tk);
-  const float2 t0 = tab[__float_as_uint(k0) & 63u], t1 = tab[__float_as_uint(k1) & 63u];
+  const uint32_t j0 = __float_as_uint(k0) & 63u, j1 = __float_as_uint(k1) & 63u;
   f2 ra, rb;
-  expf_cr_round(x, tk, f2_make(t0.x, t1.x), f2_make(t0.y, t1.y), &ra, &rb);
+  expf_cr_round(x, tk, f2_make(tab[j0], tab[j1]), f2_make(tab[64 + j0], tab[64 + j1]), &ra, &rb);
   float y0 = expf_cr_scale(f2_lo(ra), k0), y1 = expf_cr_scale(f2_hi(ra), k1);
   bool ok = ra == rb;  // both elements (64-bit compare; no zero or NaN in range)
   if (RANGE) ok = ok && fabsf(f2_lo(x)) <= kExpFastMax && fabsf(f2_hi(x)) <= kExpFastMax;

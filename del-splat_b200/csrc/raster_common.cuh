@@ -227,10 +227,14 @@ __device__ __forceinline__ float quad_y(float kC, float dy, float kb2dx, float k
   return ff(ff(kC, dy, kb2dx), dy, kadxdx);
 }
 
-// Copies expf_cr's 2^(j/64) table into the block's shared memory (one
-// barrier, at kernel start).
-__device__ __forceinline__ void load_exp_table(float2* tab) {
-  for (int i = threadIdx.x; i < 64; i += blockDim.x) tab[i] = g_exp2_64[i];
+// Copies expf_cr's 2^(j/64) table into the block's shared memory as two
+// planes, hi at [j] and rel at [64 + j] (one barrier, at kernel start).
+__device__ __forceinline__ void load_exp_table(float* tab) {
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+    const float2 t = g_exp2_64[i];
+    tab[i] = t.x;
+    tab[64 + i] = t.y;
+  }
   __syncthreads();
 }
 

@@ -26,7 +26,7 @@ namespace dsplat {
 // other pair warp-wide.  Otherwise lane L covers column L % TS, slot k at
 // row L / TS + k (32 / TS).
 template <int TS, int PPL_, bool CUDA_STOP, bool SPLIT, class Walk, class Src>
-__device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, EntP* sm, const float2* tab, float nz,
+__device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, EntP* sm, const float* tab, float nz,
                                          uint32_t s, uint32_t e, int px0, int py0, int w, int h, int xend, bool accumulate,
                                          float* __restrict__ out_rgb, size_t pix_base, float* __restrict__ out_T,
                                          uint32_t* __restrict__ out_last, const float* __restrict__ target,
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     float* __restrict__ slab_loss, uint32_t* __restrict__ item_cost, float nz) {
   using G = TaskGeo<TS, PPL, NT>;
   __shared__ EntP sm_all[kRasterWarps][32];
-  __shared__ float2 tab[64];
+  __shared__ float tab[128];
   load_exp_table(tab);
   EntP* sm = sm_all[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
     uint32_t* __restrict__ out_last, float nz) {
   using G = Geo<TS, PPL>;
   __shared__ EntP sm_all[kRasterWarps][32];
-  __shared__ float2 tab[64];
+  __shared__ float tab[128];
   load_exp_table(tab);
   EntP* sm = sm_all[threadIdx.x >> 5];
   const uint32_t task = blockIdx.x * kRasterWarps + (threadIdx.x >> 5);
