@@ -145,13 +145,24 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
             c22[q] = add2(c22[q], mul2_rn(qbl, eo2, nz2));
             T2[q] = mul2(T2[q], sub2(f2_dup(1.f), e2));
             as2[q] = add2(as2[q], eo2);
-            if (a0 && (CUDA_STOP ? f2_lo(as2[q]) >= kAlphaStop : f2_lo(as2[q]) > kAlphaStop)) {
-              live &= ~(1u << k0);
-              last[k0] = pos;
-            }
-            if (a1 && (CUDA_STOP ? f2_hi(as2[q]) >= kAlphaStop : f2_hi(as2[q]) > kAlphaStop)) {
-              live &= ~(1u << k1);
-              last[k1] = pos;
+            // a stopped slot's alpha sum is parked at -inf (it is no output),
+            // and a slot that is live but skipped keeps a sum at or below the
+            // threshold, so one test of the pair's larger sum finds every
+            // slot that stops at this entry
+            const float amax = fmaxf(f2_lo(as2[q]), f2_hi(as2[q]));
+            if (CUDA_STOP ? amax >= kAlphaStop : amax > kAlphaStop) {  // rare
+              float s0 = f2_lo(as2[q]), s1 = f2_hi(as2[q]);
+              if (CUDA_STOP ? s0 >= kAlphaStop : s0 > kAlphaStop) {
+                live &= ~(1u << k0);
+                last[k0] = pos;
+                s0 = -INFINITY;
+              }
+              if (CUDA_STOP ? s1 >= kAlphaStop : s1 > kAlphaStop) {
+                live &= ~(1u << k1);
+                last[k1] = pos;
+                s1 = -INFINITY;
+              }
+              as2[q] = f2_make(s0, s1);
             }
           }
         };
