@@ -26,7 +26,8 @@ namespace dsplat {
 // other pair warp-wide.  Otherwise lane L covers column L % TS, slot k at
 // row L / TS + k (32 / TS).
 template <int TS, int PPL_, bool CUDA_STOP, bool SPLIT, class Walk, class Src>
-__device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, EntP* sm, const float* tab, float nz,
+__device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, EntP* sm, float4* park,
+                                         uint32_t* park_pos, const float* tab, float nz,
                                          uint32_t s, uint32_t e, int px0, int py0, int w, int h, int xend, bool accumulate,
                                          float* __restrict__ out_rgb, size_t pix_base, float* __restrict__ out_T,
                                          uint32_t* __restrict__ out_last, const float* __restrict__ target,
@@ -46,7 +47,6 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
 #pragma unroll
   for (int q = 0; q < NP; ++q) fxp[q] = float(slot_x(2 * q)) + 0.5f;
   float T[PPL], as[PPL], c0[PPL], c1[PPL], c2[PPL], fy[PPL];
-  uint32_t last[PPL];
   uint32_t live = 0;
 #pragma unroll
   for (int k = 0; k < PPL; ++k) {
@@ -55,7 +55,6 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
     T[k] = 1.f;
     as[k] = 0.f;
     c0[k] = c1[k] = c2[k] = 0.f;
-    last[k] = s;
     if (ix < xend && iy < h) {
       live |= 1u << k;
       if (accumulate) {
@@ -78,9 +77,12 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
     fy2[q] = f2_make(fy[2 * q], fy[2 * q + 1]);
   }
   const f2 nz2 = f2_dup(nz);  // (-0, -0), a runtime value (see mul2_rn)
+  // a slot that stops parks its final values in the warp's shared area
+  // (park[k][lane] = T, r, g, b; park_pos[k][lane] = its stop position); its
+  // registers are no longer read, and the outputs are written after the walk
+  const uint32_t inside = live;
   // centres of the slab's first and last rows (the same for every lane)
   const float fy_first = float(py0) + 0.5f, fy_last = float(py0 + G::SLAB_ROWS - 1) + 0.5f;
-  const uint32_t inside = live;
   uint32_t hi = e;
   uint2 en = hi > s ? walk.load(hi - 1u - uint32_t(lane), uint32_t(lane) < hi - s) : make_uint2(0u, 0u);
   while (hi > s) {
@@ -127,9 +129,12 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
             // warp-uniform in practice
             const int k0 = 2 * q, k1 = 2 * q + 1;
             if (SPLIT && !(q == 0 ? cin0 : cin1)) continue;
-            const bool a0 = ((live >> k0) & 1u) && (decltype(rows)::value || (ee.z <= fy[k0] && fy[k0] <= ee.w));
-            const bool a1 = ((live >> k1) & 1u) && (decltype(rows)::value || (ee.z <= fy[k1] && fy[k1] <= ee.w));
-            if (!(a0 || a1)) continue;
+            // a0/a1: the slot's row lies in the box.  A stopped slot's
+            // registers are no longer read (its outputs are written), so only
+            // the row test masks the update
+            const bool a0 = decltype(rows)::value || (ee.z <= fy[k0] && fy[k0] <= ee.w);
+            const bool a1 = decltype(rows)::value || (ee.z <= fy[k1] && fy[k1] <= ee.w);
+            if (!((((live >> k0) & 1u) && a0) || (((live >> k1) & 1u) && a1))) continue;
             f2 adxdx2 = adxdx2_1, dx2 = dx2_1;
             if (SPLIT) col_terms(fxp[q], &adxdx2, &dx2);
             const f2 dy2 = sub2(fy2[q], qa.x);
@@ -137,29 +142,32 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
                                mul2_rn(mul2(qb.x, dy2), dy2, nz2));
             const f2 g2 = expf_cr2<!decltype(inrange)::value>(qf, tab);
             const f2 al = mul2_rn(g2, qb.y, nz2);
-            // an inactive slot of the pair takes alpha 0: its state is unchanged
-            const f2 e2 = f2_make(a0 ? f2_lo(al) : 0.f, a1 ? f2_hi(al) : 0.f);
+            // a live slot whose row is outside the box takes alpha 0: its
+            // state is unchanged
+            const f2 e2 = decltype(rows)::value ? al : f2_make(a0 ? f2_lo(al) : 0.f, a1 ? f2_hi(al) : 0.f);
             const f2 eo2 = mul2_rn(T2[q], e2, nz2);
             c02[q] = add2(c02[q], mul2_rn(qc.x, eo2, nz2));
             c12[q] = add2(c12[q], mul2_rn(qc.y, eo2, nz2));
             c22[q] = add2(c22[q], mul2_rn(qbl, eo2, nz2));
             T2[q] = mul2(T2[q], sub2(f2_dup(1.f), e2));
             as2[q] = add2(as2[q], eo2);
-            // a stopped slot's alpha sum is parked at -inf (it is no output),
-            // and a slot that is live but skipped keeps a sum at or below the
-            // threshold, so one test of the pair's larger sum finds every
-            // slot that stops at this entry
+            // a stopped slot's alpha sum is parked at -inf (it stays -inf
+            // or NaN, which no test passes), and a live slot keeps a sum at
+            // or below the threshold until it stops, so one test of the
+            // pair's larger sum finds every slot that stops at this entry
             const float amax = fmaxf(f2_lo(as2[q]), f2_hi(as2[q]));
             if (CUDA_STOP ? amax >= kAlphaStop : amax > kAlphaStop) {  // rare
               float s0 = f2_lo(as2[q]), s1 = f2_hi(as2[q]);
               if (CUDA_STOP ? s0 >= kAlphaStop : s0 > kAlphaStop) {
                 live &= ~(1u << k0);
-                last[k0] = pos;
+                park[k0 * 32 + lane] = make_float4(f2_lo(T2[q]), f2_lo(c02[q]), f2_lo(c12[q]), f2_lo(c22[q]));
+                park_pos[k0 * 32 + lane] = pos;
                 s0 = -INFINITY;
               }
               if (CUDA_STOP ? s1 >= kAlphaStop : s1 > kAlphaStop) {
                 live &= ~(1u << k1);
-                last[k1] = pos;
+                park[k1 * 32 + lane] = make_float4(f2_hi(T2[q]), f2_hi(c02[q]), f2_hi(c12[q]), f2_hi(c22[q]));
+                park_pos[k1 * 32 + lane] = pos;
                 s1 = -INFINITY;
               }
               as2[q] = f2_make(s0, s1);
@@ -185,29 +193,31 @@ __device__ __forceinline__ uint32_t fwd_slab(const Walk& walk, const Src& src, E
     if (!__any_sync(0xffffffffu, live != 0u)) break;
     __syncwarp();
   }
+  // slots still walking at the end walked the whole list (stop position s)
 #pragma unroll
   for (int q = 0; q < NP; ++q) {
-    T[2 * q] = f2_lo(T2[q]);
-    T[2 * q + 1] = f2_hi(T2[q]);
-    c0[2 * q] = f2_lo(c02[q]);
-    c0[2 * q + 1] = f2_hi(c02[q]);
-    c1[2 * q] = f2_lo(c12[q]);
-    c1[2 * q + 1] = f2_hi(c12[q]);
-    c2[2 * q] = f2_lo(c22[q]);
-    c2[2 * q + 1] = f2_hi(c22[q]);
+    if ((live >> (2 * q)) & 1u) {
+      park[2 * q * 32 + lane] = make_float4(f2_lo(T2[q]), f2_lo(c02[q]), f2_lo(c12[q]), f2_lo(c22[q]));
+      park_pos[2 * q * 32 + lane] = s;
+    }
+    if ((live >> (2 * q + 1)) & 1u) {
+      park[(2 * q + 1) * 32 + lane] = make_float4(f2_hi(T2[q]), f2_hi(c02[q]), f2_hi(c12[q]), f2_hi(c22[q]));
+      park_pos[(2 * q + 1) * 32 + lane] = s;
+    }
   }
   float l = 0.f;
 #pragma unroll
   for (int k = 0; k < PPL; ++k) {
     if (!((inside >> k) & 1u)) continue;
+    const float4 o = park[k * 32 + lane];
     const size_t p = pix_base + size_t(slot_y(k)) * w + slot_x(k);
-    out_rgb[3 * p] = c0[k];
-    out_rgb[3 * p + 1] = c1[k];
-    out_rgb[3 * p + 2] = c2[k];
-    if (out_T) out_T[p] = T[k];
-    if (out_last) out_last[p] = last[k];
+    out_rgb[3 * p] = o.y;
+    out_rgb[3 * p + 1] = o.z;
+    out_rgb[3 * p + 2] = o.w;
+    if (out_T) out_T[p] = o.x;
+    if (out_last) out_last[p] = park_pos[k * 32 + lane];
     if (target) {
-      const float d0 = c0[k] - target[3 * p], d1 = c1[k] - target[3 * p + 1], d2 = c2[k] - target[3 * p + 2];
+      const float d0 = o.y - target[3 * p], d1 = o.z - target[3 * p + 1], d2 = o.w - target[3 * p + 2];
       grad_pix[3 * p] = 2.f * d0;
       grad_pix[3 * p + 1] = 2.f * d1;
       grad_pix[3 * p + 2] = 2.f * d2;
@@ -236,9 +246,13 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     float* __restrict__ slab_loss, uint32_t* __restrict__ item_cost, float nz) {
   using G = TaskGeo<TS, PPL, NT>;
   __shared__ EntP sm_all[kRasterWarps][32];
+  __shared__ float4 park_all[kRasterWarps][G::PPL * 32];
+  __shared__ uint32_t park_pos_all[kRasterWarps][G::PPL * 32];
   __shared__ float tab[128];
   load_exp_table(tab);
   EntP* sm = sm_all[threadIdx.x >> 5];
+  float4* park = park_all[threadIdx.x >> 5];
+  uint32_t* park_pos = park_pos_all[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const uint32_t num_tasks = b.num_items * G::SLABS;
   for (;;) {
@@ -262,7 +276,7 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd(
     SbWalkSpan walk{list1, ig.lx, ig.ly, nx};
     const int xend = min(vd.w, ig.px0 + int(nx) * TS);
     const uint32_t walked = fwd_slab<G::GX, G::PPL, false, NT == 2 && G::PPL == 4>(
-        walk, src, sm, tab, nz, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, xend, false, out_rgb,
+        walk, src, sm, park, park_pos, tab, nz, ig.s, ig.e, ig.px0, ig.py0 + int(slab) * G::SLAB_ROWS, vd.w, vd.h, xend, false, out_rgb,
         vd.pix_base, out_T, out_last, target, grad_pix, slab_loss ? slab_loss + size_t(item) * G::SLABS + slab : nullptr);
     // scheduling hint for the backward and the next forward: list positions walked
     if (lane == 0 && walked) atomicMax(&item_cost[item], walked);
@@ -279,16 +293,20 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster_fwd_aos(
     uint32_t* __restrict__ out_last, float nz) {
   using G = Geo<TS, PPL>;
   __shared__ EntP sm_all[kRasterWarps][32];
+  __shared__ float4 park_all[kRasterWarps][PPL * 32];
+  __shared__ uint32_t park_pos_all[kRasterWarps][PPL * 32];
   __shared__ float tab[128];
   load_exp_table(tab);
   EntP* sm = sm_all[threadIdx.x >> 5];
+  float4* park = park_all[threadIdx.x >> 5];
+  uint32_t* park_pos = park_pos_all[threadIdx.x >> 5];
   const uint32_t task = blockIdx.x * kRasterWarps + (threadIdx.x >> 5);
   if (task >= num_tasks) return;
   const uint32_t tile = task / G::SLABS, slab = task % G::SLABS;
   const int px0 = int(tile % uint32_t(tile_w)) * TS;
   const int py0 = int(tile / uint32_t(tile_w)) * TS + int(slab) * G::SLAB_ROWS;
   TileWalk walk{idx2pnt};
-  fwd_slab<TS, PPL, CUDA_STOP, false>(walk, src, sm, tab, nz, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, w, true, pix2rgb, 0, out_T,
+  fwd_slab<TS, PPL, CUDA_STOP, false>(walk, src, sm, park, park_pos, tab, nz, tile2idx[tile], tile2idx[tile + 1], px0, py0, w, h, w, true, pix2rgb, 0, out_T,
                     out_last, nullptr, nullptr, nullptr);
 }
 
