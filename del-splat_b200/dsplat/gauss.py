@@ -66,6 +66,7 @@ class GaussBatch:
         # False keeps the forward free of host syncs (graph capture) and
         # leaves the check to the caller (status())
         self.check_overflow = bool(check_overflow)
+        self.generation = 0  # forwards issued on this batch (the autograd render checks it)
         self.n = int(num_pnt)
         self.cameras = list(cameras)
         self.tile_size = int(tile_size)
@@ -119,6 +120,7 @@ class GaussBatch:
             self.capacity, self.ws.data_ptr(), self.ws.numel(), out.data_ptr(),
             out_alpha.data_ptr() if out_alpha is not None else None,
             target.data_ptr() if target is not None else None), "batch_forward")
+        self.generation += 1
         return out
 
     def backward(self, params: Dict[str, torch.Tensor], grads: Dict[str, torch.Tensor],
@@ -228,11 +230,17 @@ class _RenderFn(torch.autograd.Function):
                     raise RuntimeError(f"tile-list capacity exceeded ({needed} entries needed, "
                                        f"{batch.capacity} available)")
         ctx.batch = batch
+        ctx.generation = batch.generation
         ctx.save_for_backward(means, log_scales, quats, opacity, colors)
         return out
 
     @staticmethod
     def backward(ctx, grad_rgb):
+        if ctx.batch.generation != ctx.generation:
+            # the batch's workspace (stop positions, final transmittance, tile
+            # lists) now holds a later forward's state
+            raise RuntimeError("render(): the batch ran another forward before this render's backward; "
+                               "call backward first or render with a separate GaussBatch")
         means, log_scales, quats, opacity, colors = ctx.saved_tensors
         params = dict(means=means.detach(), log_scales=log_scales.detach(), quats=quats.detach(),
                       opacity=opacity.detach(), colors=colors.detach())
@@ -246,7 +254,8 @@ def render(means, log_scales, quats, opacity, colors, batch: GaussBatch) -> List
 
     The backward of the returned images runs the hand-written backward
     rasteriser and projection backward.  Call backward before the next render
-    on the same batch (the forward state lives in its workspace).
+    on the same batch (the forward state lives in its workspace); a backward
+    after a later forward on the batch raises RuntimeError.
     """
     flat = _RenderFn.apply(means, log_scales, quats, opacity, colors, batch)
     return batch.images(flat)

@@ -65,6 +65,25 @@ def test_render_grows_the_lists_on_overflow(dev):
         assert torch.equal(a, b)
 
 
+def test_render_backward_after_a_later_forward_raises(dev):
+    """The forward state (stop positions, final transmittance, tile lists)
+    lives in the batch's workspace: a backward of a render that a later
+    forward on the same batch has overwritten raises instead of returning
+    the later forward's gradients; the latest render's backward still works."""
+    from dsplat.gauss import render
+    sc = _scene()
+    p = params_of(sc, dev)
+    leaves = {k: v.clone().requires_grad_(True) for k, v in p.items()}
+    batch = GaussBatch(sc.n, sc.cameras, 16, 3, pair_capacity=1 << 18, device=dev)
+    args = (leaves["means"], leaves["log_scales"], leaves["quats"], leaves["opacity"], leaves["colors"], batch)
+    first = sum(im.sum() for im in render(*args))
+    second = sum(im.sum() for im in render(*args))
+    with pytest.raises(RuntimeError, match="another forward"):
+        first.backward()
+    second.backward()
+    assert all(torch.isfinite(v.grad).all() for v in leaves.values())
+
+
 def test_fused_adam_matches_torch_optim(dev):
     torch.manual_seed(0)
     n, K = 5000, 16
