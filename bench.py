@@ -450,7 +450,7 @@ def run_zbuffer(args, rank, world, local):
     torch.cuda.synchronize()
     e2e = world * args.steps / (max_over_ranks(q0.elapsed_time(q1), world, dev) / 1e3)
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:  # the CPU baseline: rank 0 at N=1 only
         import oracle
         xyd_h = xyd.cpu().numpy()
         t0 = time.perf_counter()
@@ -685,7 +685,7 @@ def run_train4m(args, rank, world, local):
                               workload="train4m")
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:  # the CPU baseline: rank 0 at N=1 only
         try:
             nth = os.cpu_count() or 1
             t1, cam = cpu_sample(sc, 0, nth, 16)
@@ -970,7 +970,7 @@ def main():
     roofline = issue_roofline(dom, float(stage_ms[names.index(dom)]), clocks, dev, peak, peak_kind)
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:  # the CPU baseline: rank 0 at N=1 only
         try:
             nth = os.cpu_count() or 1
             rate, desc = cpu_workload_rate(base, nth, 16)  # the reference's tile size; results do not depend on it
