@@ -1,4 +1,4 @@
-"""The blend against the reference's own arithmetic (
+"""The blend against the reference's own arithmetic (the parity bar:
 images and alpha within max-abs 1e-4 of del-splat-cpu's FP32 blend).
 
 Three comparators, all on the CPU:
