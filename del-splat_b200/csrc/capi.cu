@@ -28,7 +28,7 @@ __global__ void k_adam(size_t, float*, const float*, float*, float*, float, floa
 __global__ void k_pair_cost(const ViewBatch, int, const uint32_t*, uint32_t*);
 int raster_bwd_group(int ts);
 int raster_fwd_group(int ts);
-__global__ void k_iota_pad(uint32_t*, uint32_t*, uint32_t, uint32_t, uint32_t);
+__global__ void k_pad_keys(uint32_t*, uint32_t, uint32_t, uint32_t);
 __global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*,
                            unsigned long long*);
 __global__ void k_sb_scatter(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, const uint32_t*,
@@ -53,7 +53,7 @@ size_t scan_tmp_words(size_t n);
 size_t radix_hist_words(size_t n);
 cudaError_t exclusive_scan(cudaStream_t, const uint32_t*, uint32_t*, size_t, uint32_t*);
 cudaError_t radix_sort(cudaStream_t, uint32_t*, uint32_t*, uint32_t*, uint32_t*, size_t, const uint32_t*, int, uint32_t,
-                       uint32_t*, uint32_t*, bool*, const uint2*, uint32_t, uint2*);
+                       uint32_t*, uint32_t*, bool*, const uint2*, uint32_t, uint2*, bool, uint32_t);
 cudaError_t raster_fwd(cudaStream_t, const ViewBatch&, const FwdArgs&);
 cudaError_t raster_bwd(cudaStream_t, const ViewBatch&, const BwdArgs&);
 bool raster_config_ok(int ts, int ppl);
@@ -362,14 +362,16 @@ int tiles_fill(cudaStream_t st, uint32_t n, const float* xyd, const float* aabb,
   }
   const uint32_t npad = ceil_div(n, kSortTile) * kSortTile;
   ViewBatch b = single_view_batch(img_w, img_h, int(ts), tile_w, tile_h);
-  k_iota_pad<<<blocks_for(npad, 256), 256, 0, st>>>(t.dva, t.dka, n, npad, 1);
-  count_launch();
+  if (npad > n) {
+    k_pad_keys<<<blocks_for(npad - n, 256), 256, 0, st>>>(t.dka, n, npad, 1);
+    count_launch();
+  }
   k_prep_tiles<<<blocks_for(n, 256), 256, 0, st>>>(n, xyd, aabb, rad, int(ts), int(tile_w), int(tile_h), t.rect,
                                                   t.dka, t.cnt);
   count_launch();
   bool in_b = false;
   TRY_CUDA(radix_sort(st, t.dka, t.dva, t.dkb, t.dvb, npad, nullptr, 32, 1, t.hist, t.scan_tmp, &in_b, t.rect, n,
-                      t.srect),
+                      t.srect, true, n),
            "depth sort");
   const uint32_t* order = in_b ? t.dvb : t.dva;
   int rc = build_sb_lists(st, b, n, npad, order, t.srect, t.lists, t.scan_tmp, capacity, t.flags);
@@ -726,8 +728,10 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
   if (n == 0 || pair_capacity == 0) {
     TRY_CUDA(cudaMemsetAsync(w.lists.off1, 0, (size_t(b.num_sb) * (npad / kChunk) + 1) * 4, st), "memset");
   } else {
-    k_iota_pad<<<blocks_for(Vp, 256), 256, 0, st>>>(w.dva, w.dka, n, npad, V);
-    count_launch();
+    if (npad > n) {
+      k_pad_keys<<<blocks_for(size_t(npad - n) * V, 256), 256, 0, st>>>(w.dka, n, npad, V);
+      count_launch();
+    }
     k_fused_project<<<blocks_for(n, 128), 128, 0, st>>>(n, npad, params->sh_degree, params->means,
                                                         params->log_scales, params->quats, params->opacity,
                                                         params->colors, b, w.rec, w.rect, w.dka, nullptr);
@@ -735,7 +739,7 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
     stage_mark(st, 1);
     bool in_b = false;
     TRY_CUDA(radix_sort(st, w.dka, w.dva, w.dkb, w.dvb, Vp, nullptr, 32, V, w.hist, w.scan_tmp, &in_b, w.rect, n,
-                        w.srect),
+                        w.srect, true, n),
              "depth sort");
     stage_mark(st, 2);
     const uint32_t* order = in_b ? w.dvb : w.dva;

@@ -179,7 +179,7 @@ __device__ __forceinline__ uint32_t peers_of_digit(uint32_t d) {
 __global__ void __launch_bounds__(kRsThreads) k_radix_downsweep(
     const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
     uint32_t* __restrict__ vout, int shift, uint32_t nb_seg, const uint32_t* __restrict__ offs, int write_keys,
-    const uint2* __restrict__ gather_src, uint32_t gather_n, uint2* __restrict__ gather_dst) {
+    const uint2* __restrict__ gather_src, uint32_t gather_n, uint2* __restrict__ gather_dst, uint32_t iota_n) {
   __shared__ uint32_t wc[kRsWarps][256];
   __shared__ uint32_t dstart[256];
   __shared__ uint32_t goff[256];
@@ -192,10 +192,22 @@ __global__ void __launch_bounds__(kRsThreads) k_radix_downsweep(
   const uint32_t lt = (1u << lane) - 1u;
   const size_t base = size_t(blockIdx.x) * kRsTile + size_t(warp) * (kRsRounds * 32);
   uint32_t k[kRsRounds], v[kRsRounds];
+  // vin null (first pass of a sort of the identity permutation): an
+  // element's value is its index in its segment, 0xffffffff from iota_n on
+  if (vin) {
 #pragma unroll
-  for (int r = 0; r < kRsRounds; ++r) {
-    k[r] = kin[base + r * 32 + lane];
-    v[r] = vin[base + r * 32 + lane];
+    for (int r = 0; r < kRsRounds; ++r) {
+      k[r] = kin[base + r * 32 + lane];
+      v[r] = vin[base + r * 32 + lane];
+    }
+  } else {
+    const uint32_t local0 = (blockIdx.x % nb_seg) * kRsTile + uint32_t(warp) * (kRsRounds * 32) + uint32_t(lane);
+#pragma unroll
+    for (int r = 0; r < kRsRounds; ++r) {
+      k[r] = kin[base + r * 32 + lane];
+      const uint32_t local = local0 + uint32_t(r) * 32u;
+      v[r] = local < iota_n ? local : 0xffffffffu;
+    }
   }
   // phase 1: per-warp digit counts (the peer masks are kept for phase 3)
   uint32_t pm[kRsRounds];
@@ -268,9 +280,13 @@ size_t radix_hist_words(size_t n) { return ((n + kRsTile - 1) / kRsTile) * 256; 
 // null (every element takes part).
 // gather_dst (nullable): the last pass also writes, per sorted position,
 // gather_src[segment * gather_n + value] (an empty record for padding).
+// iota_values: the values are the identity permutation (each segment's
+// element indices, 0xffffffff from iota_n on); va is not read, the first pass
+// forms them.
 cudaError_t radix_sort(cudaStream_t st, uint32_t* ka, uint32_t* va, uint32_t* kb, uint32_t* vb, size_t n,
                        const uint32_t* count_ptr, int nbits, uint32_t nseg, uint32_t* hist, uint32_t* scan_tmp,
-                       bool* result_in_b, const uint2* gather_src, uint32_t gather_n, uint2* gather_dst) {
+                       bool* result_in_b, const uint2* gather_src, uint32_t gather_n, uint2* gather_dst,
+                       bool iota_values, uint32_t iota_n) {
   if (n % kRsTile != 0 || count_ptr != nullptr || nseg == 0 || (n / kRsTile) % nseg != 0)
     return cudaErrorInvalidValue;
   const uint32_t nblocks = uint32_t(n / kRsTile);
@@ -283,7 +299,7 @@ cudaError_t radix_sort(cudaStream_t st, uint32_t* ka, uint32_t* va, uint32_t* kb
   }
   for (int shift = 0; shift < nbits; shift += 8) {
     const uint32_t* ki = in_b ? kb : ka;
-    const uint32_t* vi = in_b ? vb : va;
+    const uint32_t* vi = iota_values && shift == 0 ? nullptr : in_b ? vb : va;
     uint32_t* ko = in_b ? ka : kb;
     uint32_t* vo = in_b ? va : vb;
     k_radix_upsweep<<<nblocks, kRsThreads, 0, st>>>(ki, shift, nb_seg, hist); count_launch();
@@ -291,7 +307,7 @@ cudaError_t radix_sort(cudaStream_t st, uint32_t* ka, uint32_t* va, uint32_t* kb
     if (e != cudaSuccess) return e;
     const int last = shift + 8 >= nbits;
     k_radix_downsweep<<<nblocks, kRsThreads, 0, st>>>(ki, vi, ko, vo, shift, nb_seg, hist, last ? 0 : 1,
-                                                       gather_src, gather_n, last ? gather_dst : nullptr);
+                                                       gather_src, gather_n, last ? gather_dst : nullptr, iota_n);
     count_launch();
     in_b = !in_b;
   }
@@ -302,13 +318,13 @@ cudaError_t radix_sort(cudaStream_t st, uint32_t* ka, uint32_t* va, uint32_t* kb
 // ---------------------------------------------------------------------------
 // Rank order helpers
 // ---------------------------------------------------------------------------
-__global__ void k_iota_pad(uint32_t* __restrict__ vals, uint32_t* __restrict__ keys, uint32_t n, uint32_t npad,
-                           uint32_t nseg) {
+// Keys of the padding elements [n, npad) of every segment: 0xffffffff (they
+// sort last; their values are formed by the sort's first pass).
+__global__ void k_pad_keys(uint32_t* __restrict__ keys, uint32_t n, uint32_t npad, uint32_t nseg) {
+  const uint32_t pad = npad - n;
   const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= size_t(npad) * nseg) return;
-  const uint32_t r = uint32_t(i % npad);
-  vals[i] = r < n ? r : 0xffffffffu;
-  if (r >= n) keys[i] = 0xffffffffu;
+  if (i >= size_t(pad) * nseg) return;
+  keys[size_t(i / pad) * npad + n + uint32_t(i % pad)] = 0xffffffffu;
 }
 
 // superblock span of a tile span (superblocks of 1 << sl tiles per side);
