@@ -26,7 +26,6 @@ __global__ void k_project_bwd_colour(uint32_t, int, const float*, const float*, 
 __global__ void k_prepare_grad2d(const unsigned long long*, unsigned long long, float4*, size_t);
 __global__ void k_adam(size_t, float*, const float*, float*, float*, float, float, float, float, float, float);
 __global__ void k_pair_cost(const ViewBatch, int, const uint32_t*, uint32_t*);
-int raster_bwd_group(int ts);
 int raster_fwd_group(int ts);
 __global__ void k_pad_keys(uint32_t*, uint32_t, uint32_t, uint32_t);
 __global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*,
@@ -405,7 +404,7 @@ struct BatchWs {
   float* slab_loss;
   float4* grad2d;
   unsigned long long* grad2d_tag;  // == grad2d_tag_value(): grad2d is all zero
-  uint32_t *sched, *task_order, *task_order_bwd, *item_cost, *pair_cost;
+  uint32_t *sched, *task_order, *item_cost, *pair_cost;
 };
 
 int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, int32_t ppl, ViewBatch* b) {
@@ -498,7 +497,6 @@ BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity)
   w.grad2d_tag = c.take<unsigned long long>(1);
   w.sched = c.take<uint32_t>(80);
   w.task_order = c.take<uint32_t>(size_t(b.num_items) + 1);
-  w.task_order_bwd = c.take<uint32_t>(size_t(b.num_items) + 1);
   w.item_cost = c.take<uint32_t>(size_t(b.num_items) + 1);
   w.pair_cost = c.take<uint32_t>(size_t(b.num_items) + 1);
   L.total_bytes = align_up(c.off, 256);
@@ -798,17 +796,12 @@ int dsplat_gauss_batch_backward(dsplat_stream stream, const dsplat_gauss_params*
       w.grad2d_tag, tag, w.grad2d, 3 * VN);
   count_launch();
   TRY_CUDA(cudaMemsetAsync(w.flags + 3, 0, sizeof(uint32_t), st), "memset");
-  // longest-first order from this forward's measured walks
-  const uint32_t* bwd_cost = w.item_cost;
-  if (raster_bwd_group(b.ts) > 1) {
-    k_pair_cost<<<64, 256, 0, st>>>(b, raster_bwd_group(b.ts), w.item_cost, w.pair_cost);
-    count_launch();
-    bwd_cost = w.pair_cost;
-  }
-  TRY_CUDA(order_tasks(st, b, w.lists.off1, w.L.npad / kChunk, bwd_cost, w.sched, w.task_order_bwd), "task order");
+  // the forward's longest-first task order: it ranks the tasks by the walks
+  // of the forward before it, the same measure as this forward's (equal once
+  // the scene stops changing), and every order gives the same results
   stage_mark(st, 7);
   const BwdArgs ba{n,           w.rec,    w.lists.list1,  w.lists.off1, w.L.npad / kChunk, pair_capacity,
-                   w.task_order_bwd, w.flags + 3, grad_rgb ? grad_rgb : w.grad_pix, w.pix_T, w.pix_stop, w.grad2d};
+                   w.task_order, w.flags + 3, grad_rgb ? grad_rgb : w.grad_pix, w.pix_T, w.pix_stop, w.grad2d};
   TRY_CUDA(raster_bwd(st, b, ba),
            "raster_bwd");
   stage_mark(st, 8);

@@ -245,8 +245,6 @@ static void launch_bwd(cudaStream_t st, const ViewBatch& b, const BwdArgs& a) {
   count_launch();
 }
 
-// tiles per backward task (see k_raster_bwd): 2 for 8x8 tiles
-int raster_bwd_group(int ts) { return ts == 8 ? kBwdGroup8 : 1; }
 
 cudaError_t raster_bwd(cudaStream_t st, const ViewBatch& b, const BwdArgs& a) {
 #define X(T, P)                        \

@@ -59,6 +59,7 @@ namespace dsplat {
 constexpr int kRasterWarps = 4;  // warps per CTA (independent tasks)
 constexpr int kFwdGroup8 = 2;    // 8x8 tiles per forward task
 constexpr int kBwdGroup8 = 2;    // 8x8 tiles per backward task (4 measured slower: registers, partial overlaps)
+static_assert(kFwdGroup8 == kBwdGroup8, "the backward runs its tasks in the forward's order");
 
 // The backward evaluates exp(-q/2) as 2^(k q) with k = -log2(e)/2 folded
 // into the staged conic (hardware ex2.approx; see k_raster_bwd).
