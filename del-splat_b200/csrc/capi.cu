@@ -25,7 +25,6 @@ __global__ void k_project_bwd_colour(uint32_t, int, const float*, const float*, 
                                      float*, float*, unsigned long long*, unsigned long long);
 __global__ void k_prepare_grad2d(const unsigned long long*, unsigned long long, float4*, size_t);
 __global__ void k_adam(size_t, float*, const float*, float*, float*, float, float, float, float, float, float);
-__global__ void k_pair_cost(const ViewBatch, int, const uint32_t*, uint32_t*);
 int raster_fwd_group(int ts);
 __global__ void k_pad_keys(uint32_t*, uint32_t, uint32_t, uint32_t);
 __global__ void k_sb_count(const uint32_t*, const uint2*, uint32_t, uint32_t, const ViewBatch, uint32_t*,
@@ -58,9 +57,10 @@ cudaError_t raster_bwd(cudaStream_t, const ViewBatch&, const BwdArgs&);
 bool raster_config_ok(int ts, int ppl);
 int raster_default_ppl(int ts);
 uint32_t raster_slabs_per_tile(int ts, int ppl);
-__global__ void k_order_hist(const ViewBatch, const uint32_t*, uint32_t, const uint32_t*, uint32_t*);
+__global__ void k_order_hist(const ViewBatch, const uint32_t*, uint32_t, const uint32_t*, int, uint32_t*);
 __global__ void k_order_scan(uint32_t*);
-__global__ void k_order_scatter(const ViewBatch, const uint32_t*, uint32_t, const uint32_t*, uint32_t*, uint32_t*);
+__global__ void k_order_scatter(const ViewBatch, const uint32_t*, uint32_t, const uint32_t*, int, uint32_t*,
+                                uint32_t*);
 cudaError_t raster_fwd_aos(cudaStream_t, int, int, int, float*, const float*, const float*, const float*, const float*,
                            const float*, const uint32_t*, const uint32_t*, float*, uint32_t*, bool);
 cudaError_t expf_cr_launch(cudaStream_t, size_t, const float*, float*);
@@ -214,14 +214,14 @@ int build_tile_lists(cudaStream_t st, const ViewBatch& b, uint32_t npad, const L
 }
 
 cudaError_t order_tasks(cudaStream_t st, const ViewBatch& b, const uint32_t* off1, uint32_t nchunk,
-                        const uint32_t* cost, uint32_t* sched, uint32_t* order) {
+                        const uint32_t* cost, int nt, uint32_t* sched, uint32_t* order) {
   cudaError_t e = cudaMemsetAsync(sched, 0, 80 * sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
-  k_order_hist<<<296, 256, 0, st>>>(b, off1, nchunk, cost, sched);
+  k_order_hist<<<296, 256, 0, st>>>(b, off1, nchunk, cost, nt, sched);
   count_launch();
   k_order_scan<<<1, 32, 0, st>>>(sched);
   count_launch();
-  k_order_scatter<<<296, 256, 0, st>>>(b, off1, nchunk, cost, sched, order);
+  k_order_scatter<<<296, 256, 0, st>>>(b, off1, nchunk, cost, nt, sched, order);
   count_launch();
   return cudaGetLastError();
 }
@@ -404,7 +404,7 @@ struct BatchWs {
   float* slab_loss;
   float4* grad2d;
   unsigned long long* grad2d_tag;  // == grad2d_tag_value(): grad2d is all zero
-  uint32_t *sched, *task_order, *item_cost, *pair_cost;
+  uint32_t *sched, *task_order, *item_cost;
 };
 
 int make_batch(int64_t n64, int32_t nv, const dsplat_view* views, int32_t ts, int32_t ppl, ViewBatch* b) {
@@ -498,7 +498,6 @@ BatchWs carve_batch(void* ws, uint32_t n, const ViewBatch& b, uint64_t capacity)
   w.sched = c.take<uint32_t>(80);
   w.task_order = c.take<uint32_t>(size_t(b.num_items) + 1);
   w.item_cost = c.take<uint32_t>(size_t(b.num_items) + 1);
-  w.pair_cost = c.take<uint32_t>(size_t(b.num_items) + 1);
   L.total_bytes = align_up(c.off, 256);
   return w;
 }
@@ -746,13 +745,9 @@ int dsplat_gauss_batch_forward(dsplat_stream stream, const dsplat_gauss_params* 
     stage_mark(st, 3);
   }
   // longest-first raster task order (costs measured by the previous forward)
-  const uint32_t* fwd_cost = w.item_cost;
-  if (raster_fwd_group(b.ts) > 1) {
-    k_pair_cost<<<64, 256, 0, st>>>(b, raster_fwd_group(b.ts), w.item_cost, w.pair_cost);
-    count_launch();
-    fwd_cost = w.pair_cost;
-  }
-  TRY_CUDA(order_tasks(st, b, w.lists.off1, npad / kChunk, fwd_cost, w.sched, w.task_order), "task order");
+  TRY_CUDA(order_tasks(st, b, w.lists.off1, npad / kChunk, w.item_cost, raster_fwd_group(b.ts), w.sched,
+                       w.task_order),
+           "task order");
   TRY_CUDA(cudaMemsetAsync(w.item_cost, 0, size_t(b.num_items) * sizeof(uint32_t), st), "memset");
   stage_mark(st, 4);
   const FwdArgs fa{n,           w.rec,   w.lists.list1, w.lists.off1, npad / kChunk, pair_capacity, w.task_order,

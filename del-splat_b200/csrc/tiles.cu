@@ -753,28 +753,34 @@ __global__ void __launch_bounds__(kMsThreads) k_tile_scatter(const uint2* __rest
 // none is recorded yet, its superblock-list length.  Only the schedule
 // depends on it, never the results.  sched[0..32] counts, [40..72] cursors.
 // ---------------------------------------------------------------------------
+// Longest-first bucket of an item (0 = longest): clz of the list positions
+// its task walked in the previous forward (cost[item]), else of its
+// superblock's list length.  With nt > 1 adjacent tiles per task (8x8
+// tiles) only a group's leading tile leads a task and carries its cost; the
+// other tiles lead none (their tasks return at once) and go last.
 __device__ __forceinline__ uint32_t item_cost_bucket(const ViewBatch& b, uint32_t item, const uint32_t* off1,
-                                                     uint32_t nchunk, const uint32_t* cost) {
-  const uint32_t measured = cost ? cost[item] : 0u;
-  if (measured) return uint32_t(__clz(measured));
+                                                     uint32_t nchunk, const uint32_t* cost, int nt) {
   int v = 0;
   for (int k = 1; k < b.num_views; ++k)
     if (item >= b.v[k].item_base) v = k;
   const ViewDev& vd = b.v[v];
   const uint32_t t = item - vd.item_base;
   const uint32_t tx = t % uint32_t(vd.tile_w), ty = t / uint32_t(vd.tile_w);
+  if (nt > 1 && tx % min(uint32_t(nt), 1u << vd.sb_log2)) return 31u;
+  const uint32_t measured = cost ? cost[item] : 0u;
+  if (measured) return uint32_t(__clz(measured));
   const uint32_t sb = vd.sb_base + (ty >> vd.sb_log2) * uint32_t(sb_cols(vd)) + (tx >> vd.sb_log2);
   const uint32_t len = off1[size_t(sb + 1) * nchunk] - off1[size_t(sb) * nchunk];
-  return len ? uint32_t(__clz(len)) : 32u;  // 0 = longest
+  return len ? uint32_t(__clz(len)) : 32u;
 }
 
 __global__ void k_order_hist(const ViewBatch b, const uint32_t* __restrict__ off1, uint32_t nchunk,
-                             const uint32_t* __restrict__ cost, uint32_t* __restrict__ sched) {
+                             const uint32_t* __restrict__ cost, int nt, uint32_t* __restrict__ sched) {
   __shared__ uint32_t h[33];
   if (threadIdx.x < 33) h[threadIdx.x] = 0;
   __syncthreads();
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.num_items; i += gridDim.x * blockDim.x)
-    atomicAdd(&h[item_cost_bucket(b, i, off1, nchunk, cost)], 1u);
+    atomicAdd(&h[item_cost_bucket(b, i, off1, nchunk, cost, nt)], 1u);
   __syncthreads();
   if (threadIdx.x < 33 && h[threadIdx.x]) atomicAdd(&sched[threadIdx.x], h[threadIdx.x]);
 }
@@ -793,7 +799,7 @@ __global__ void k_order_scan(uint32_t* __restrict__ sched) {
 // takes one range per bucket from the global cursors (one global atomic per
 // bucket and block instead of one per item on 33 hot counters).
 __global__ void k_order_scatter(const ViewBatch b, const uint32_t* __restrict__ off1, uint32_t nchunk,
-                                const uint32_t* __restrict__ cost, uint32_t* __restrict__ sched,
+                                const uint32_t* __restrict__ cost, int nt, uint32_t* __restrict__ sched,
                                 uint32_t* __restrict__ order) {
   __shared__ uint32_t cnt[33], base[33];
   const uint32_t per_block = (b.num_items + gridDim.x - 1) / gridDim.x;
@@ -804,7 +810,7 @@ __global__ void k_order_scatter(const ViewBatch b, const uint32_t* __restrict__ 
     const uint32_t i = i0 + threadIdx.x;
     uint32_t bucket = 0, slot = 0;
     if (i < hi) {
-      bucket = item_cost_bucket(b, i, off1, nchunk, cost);
+      bucket = item_cost_bucket(b, i, off1, nchunk, cost, nt);
       slot = atomicAdd(&cnt[bucket], 1u);
     }
     __syncthreads();
@@ -815,28 +821,6 @@ __global__ void k_order_scatter(const ViewBatch b, const uint32_t* __restrict__ 
   }
 }
 
-// Costs for the grouped backward (nt adjacent tiles of a superblock row per
-// task, fewer where the superblock is narrower): a group costs the longest
-// of its tiles' walks; the other tiles of a group lead no task (cost 1:
-// ordered among the cheapest; their tasks return at once).
-__global__ void k_pair_cost(const ViewBatch b, int nt, const uint32_t* __restrict__ cost,
-                            uint32_t* __restrict__ pair_cost) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.num_items; i += gridDim.x * blockDim.x) {
-    int v = 0;
-    for (int k = 1; k < b.num_views; ++k)
-      if (i >= b.v[k].item_base) v = k;
-    const ViewDev& vd = b.v[v];
-    const uint32_t tx = (i - vd.item_base) % uint32_t(vd.tile_w);
-    const uint32_t nx = min(uint32_t(nt), 1u << vd.sb_log2);
-    uint32_t c = cost[i];
-    if (tx % nx) {
-      c = 1u;
-    } else {
-      for (uint32_t k = 1; k < nx && tx + k < uint32_t(vd.tile_w); ++k) c = max(c, cost[i + k]);
-    }
-    pair_cost[i] = c;
-  }
-}
 
 // Clamp tile ranges to the pair capacity after an overflow so that readers
 // stay in bounds (the results are then invalid and the flag is set).
