@@ -58,7 +58,6 @@ bool raster_config_ok(int ts, int ppl);
 int raster_default_ppl(int ts);
 uint32_t raster_slabs_per_tile(int ts, int ppl);
 __global__ void k_order_hist(const ViewBatch, const uint32_t*, uint32_t, const uint32_t*, int, uint32_t*);
-__global__ void k_order_scan(uint32_t*);
 __global__ void k_order_scatter(const ViewBatch, const uint32_t*, uint32_t, const uint32_t*, int, uint32_t*,
                                 uint32_t*);
 cudaError_t raster_fwd_aos(cudaStream_t, int, int, int, float*, const float*, const float*, const float*, const float*,
@@ -218,8 +217,6 @@ cudaError_t order_tasks(cudaStream_t st, const ViewBatch& b, const uint32_t* off
   cudaError_t e = cudaMemsetAsync(sched, 0, 80 * sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
   k_order_hist<<<296, 256, 0, st>>>(b, off1, nchunk, cost, nt, sched);
-  count_launch();
-  k_order_scan<<<1, 32, 0, st>>>(sched);
   count_launch();
   k_order_scatter<<<296, 256, 0, st>>>(b, off1, nchunk, cost, nt, sched, order);
   count_launch();

@@ -26,7 +26,8 @@
 namespace dsplat {
 
 // ---------------------------------------------------------------------------
-// Exclusive scan of u32 (three kernels; any length).
+// Exclusive scan of u32 (two kernels: block totals, then each block adds the
+// earlier blocks' totals to its own scan; any length).
 // ---------------------------------------------------------------------------
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 8;
@@ -74,24 +75,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const uint32_t* __
   if (threadIdx.x == 0) sums[blockIdx.x] = tot;
 }
 
-// single block: exclusive scan of the block sums, any count
-__global__ void __launch_bounds__(kScanThreads) k_scan_sums(uint32_t* sums, uint32_t nb) {
-  __shared__ uint32_t carry_s;
-  __shared__ uint32_t tot;
-  if (threadIdx.x == 0) carry_s = 0;
-  __syncthreads();
-  for (uint32_t base = 0; base < nb; base += kScanThreads) {
-    const uint32_t i = base + threadIdx.x;
-    uint32_t x = i < nb ? sums[i] : 0u;
-    uint32_t p = block_excl_scan(x, &tot);
-    const uint32_t c = carry_s;
-    if (i < nb) sums[i] = c + p;
-    __syncthreads();
-    if (threadIdx.x == 0) carry_s = c + tot;
-    __syncthreads();
-  }
-}
-
 __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const uint32_t* __restrict__ in,
                                                              uint32_t* __restrict__ out, size_t n,
                                                              const uint32_t* __restrict__ sums) {
@@ -103,8 +86,13 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const uint32_t* __r
     v[i] = base + i < n ? in[base + i] : 0u;
     s += v[i];
   }
-  __shared__ uint32_t tot;
-  uint32_t p = block_excl_scan(s, &tot) + sums[blockIdx.x];
+  // the earlier blocks' totals, summed by every block itself (a few hundred
+  // words for the scans here, so no separate pass scans them)
+  uint32_t part = 0;
+  for (uint32_t i = threadIdx.x; i < blockIdx.x; i += kScanThreads) part += sums[i];
+  __shared__ uint32_t carry, tot;
+  block_excl_scan(part, &carry);
+  uint32_t p = block_excl_scan(s, &tot) + carry;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     if (base + i < n) out[base + i] = p;
@@ -118,7 +106,6 @@ cudaError_t exclusive_scan(cudaStream_t st, const uint32_t* in, uint32_t* out, s
   if (n == 0) return cudaSuccess;
   const uint32_t nb = uint32_t((n + kScanTile - 1) / kScanTile);
   k_scan_reduce<<<nb, kScanThreads, 0, st>>>(in, n, tmp); count_launch();
-  k_scan_sums<<<1, kScanThreads, 0, st>>>(tmp, nb); count_launch();
   k_scan_apply<<<nb, kScanThreads, 0, st>>>(in, out, n, tmp); count_launch();
   return cudaGetLastError();
 }
@@ -785,23 +772,23 @@ __global__ void k_order_hist(const ViewBatch b, const uint32_t* __restrict__ off
   if (threadIdx.x < 33 && h[threadIdx.x]) atomicAdd(&sched[threadIdx.x], h[threadIdx.x]);
 }
 
-__global__ void k_order_scan(uint32_t* __restrict__ sched) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    uint32_t run = 0;
-    for (int k = 0; k < 33; ++k) {
-      sched[40 + k] = run;
-      run += sched[k];
-    }
-  }
-}
-
 // Scatter into bucket order: each block ranks its items in shared memory and
 // takes one range per bucket from the global cursors (one global atomic per
-// bucket and block instead of one per item on 33 hot counters).
+// bucket and block instead of one per item on 33 hot counters).  sched[0..33)
+// holds the bucket counts, sched[40..73) the cursors (zero at the start);
+// every block forms the buckets' starts from the counts itself.
 __global__ void k_order_scatter(const ViewBatch b, const uint32_t* __restrict__ off1, uint32_t nchunk,
                                 const uint32_t* __restrict__ cost, int nt, uint32_t* __restrict__ sched,
                                 uint32_t* __restrict__ order) {
-  __shared__ uint32_t cnt[33], base[33];
+  __shared__ uint32_t cnt[33], base[33], start[33];
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (int k = 0; k < 33; ++k) {
+      start[k] = run;
+      run += sched[k];
+    }
+  }
+  __syncthreads();
   const uint32_t per_block = (b.num_items + gridDim.x - 1) / gridDim.x;
   const uint32_t lo = blockIdx.x * per_block, hi = min(b.num_items, lo + per_block);
   for (uint32_t i0 = lo; i0 < hi; i0 += blockDim.x) {
@@ -814,7 +801,8 @@ __global__ void k_order_scatter(const ViewBatch b, const uint32_t* __restrict__ 
       slot = atomicAdd(&cnt[bucket], 1u);
     }
     __syncthreads();
-    if (threadIdx.x < 33 && cnt[threadIdx.x]) base[threadIdx.x] = atomicAdd(&sched[40 + threadIdx.x], cnt[threadIdx.x]);
+    if (threadIdx.x < 33 && cnt[threadIdx.x])
+      base[threadIdx.x] = start[threadIdx.x] + atomicAdd(&sched[40 + threadIdx.x], cnt[threadIdx.x]);
     __syncthreads();
     if (i < hi) order[base[bucket] + slot] = i;
     __syncthreads();
